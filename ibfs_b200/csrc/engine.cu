@@ -1,0 +1,1044 @@
+// engine.cu -- kernels, the resident-graph handle and the ibfs_run schedules.
+//
+// Two schedules over the same phase functions (bfs_device.cuh):
+//   PLAIN       host-driven level loop: one launch per phase and a host
+//               synchronisation per level to read the counters -- the shape
+//               of the reference's ibfs() loop (bfs_gpu_opt.cuh:99-166);
+//   PERSISTENT  one cooperative launch runs every level of every batch: the
+//               grid is cut into G groups of CTAs, each group owns one batch
+//               at a time and synchronises with a bounded team barrier; the
+//               direction decision is taken on the device.  Optionally the
+//               whole run (uploads, launch, downloads) is captured once in a
+//               CUDA graph and replayed.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "bfs_device.cuh"
+#include "internal.h"
+
+namespace ibfs {
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ Team make_team(int block, int nblocks) {
+  Team t;
+  t.block = block;
+  t.nblocks = nblocks;
+  t.tid = (long long)block * blockDim.x + threadIdx.x;
+  t.nthreads = (long long)nblocks * blockDim.x;
+  t.warp = t.tid >> 5;
+  t.nwarps = t.nthreads >> 5;
+  t.lane = threadIdx.x & 31;
+  return t;
+}
+
+__device__ __forceinline__ void zero_words(uint32_t* p, long long nwords, const Team& t) {
+  // nwords is a multiple of 4 and p 16-byte aligned (allocation padding)
+  uint4* q = reinterpret_cast<uint4*>(p);
+  const uint4 z = make_uint4(0, 0, 0, 0);
+  for (long long i = t.tid; i < nwords / 4; i += t.nthreads) __stcg(q + i, z);
+}
+
+__device__ __forceinline__ int depth_limit(int db) { return db == 1 ? 254 : 65534; }
+
+__device__ __forceinline__ uint8_t* batch_depth(const Params& p, const GroupBufs& gb, int b) {
+  return p.layout == 1 ? p.out + (size_t)b * (size_t)p.V * p.C * p.db : gb.stage;
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
+  extern __shared__ __align__(16) uint8_t dsmem[];
+  __shared__ int s_dir, s_stop, s_err;
+  const int g = blockIdx.x / p.cpg;
+  const Team t = make_team(blockIdx.x % p.cpg, p.cpg);
+  const GroupBufs gb = p.groups[g];
+  Ctl* ctl = gb.ctl;
+  const unsigned nb = (unsigned)p.cpg;
+  const bool lead = (t.block == 0 && threadIdx.x == 0);
+  bool withhold = p.withhold && t.block == 0 && g == 0;
+  const long long vpad = (p.V + 31) & ~31LL;
+  const long long nchg_pad = (p.nchg + 3) & ~3LL;
+
+#define BARRIER()                                                   \
+  do {                                                              \
+    if (!team_barrier(ctl, nb, p.timeout_ns, withhold)) return;     \
+    withhold = false;                                               \
+  } while (0)
+
+  for (int b = g; b < p.nbatches; b += p.G) {
+    const long long k0 = (long long)b * p.C;
+    const int n_b = (int)min((long long)p.C, p.n_total - k0);
+    uint8_t* depth = batch_depth(p, gb, b);
+    zero_words(gb.last, vpad * WORDS, t);
+    zero_words(gb.curr, vpad * WORDS, t);
+    zero_words(gb.chg, nchg_pad, t);
+    if (lead) {
+      memset(&ctl->par[0], 0, sizeof(Par) * 2);
+      memset(&ctl->qc[0][0], 0, sizeof(ctl->qc));
+    }
+    BARRIER();
+    seed_phase<WORDS>(p, gb, p.src + k0, n_b, t);
+    BARRIER();
+    inspect_phase<WORDS>(p, gb, &ctl->par[0], depth, n_b, 0, true, t);
+    BARRIER();
+    int level = 0, cur_dir = kDirTD, max_level = 0, td = 0, bu = 0;
+    unsigned long long m_u = (unsigned long long)p.E, teps = 0;
+    int err = 0;
+    while (true) {
+      if (threadIdx.x == 0) {
+        const volatile Par* pr = &ctl->par[level & 1];
+        const unsigned long long changed = pr->changed, mf = pr->mf, cdeg = pr->cdeg;
+        teps += pr->teps;
+        m_u = m_u > cdeg ? m_u - cdeg : 0ull;
+        int stop = 0;
+        if (pr->range_err) { stop = 1; err = 3; }
+        else if (changed == 0) stop = 1;
+        else if (level + 1 > p.max_levels) { stop = 1; err = 3; }
+        if (changed && !pr->range_err) max_level = level;
+        int nd = choose_dir(level + 1, cur_dir, p.switch_level, p.alpha, p.beta,
+                            changed, mf, m_u, p.V);
+        if (t.block == 0) {
+          if (b < p.nbatches && level < p.lrec_cap) {
+            LevelRec r;
+            r.batch = b; r.level = level; r.dir = level == 0 ? -1 : cur_dir; r.pad = 0;
+            r.frontier = (long long)changed; r.frontier_edges = (long long)mf;
+            p.lrec[(size_t)b * p.lrec_cap + level] = r;
+          }
+          if (!stop) {
+            memset((void*)&ctl->par[(level + 1) & 1], 0, sizeof(Par));
+            ctl->qc[level & 1][0] = ctl->qc[level & 1][1] = ctl->qc[level & 1][2] = 0;
+          }
+        }
+        s_dir = nd;
+        s_stop = stop;
+        s_err = err;
+      }
+      __syncthreads();
+      const int stop = s_stop;
+      cur_dir = s_dir;
+      err = s_err;
+      __syncthreads();
+      if (stop) break;
+      level++;
+      if (cur_dir == kDirTD) {
+        td++;
+        qbuild_phase(p, gb, ctl->qc[level & 1], t);
+        BARRIER();
+        td_phase<WORDS>(p, gb, ctl->qc[level & 1], t);
+      } else {
+        bu++;
+        bu_phase<WORDS>(p, gb, ctl->par[(level - 1) & 1].fmask, t);
+      }
+      BARRIER();
+      inspect_phase<WORDS>(p, gb, &ctl->par[level & 1], depth, n_b, level,
+                           level <= depth_limit(p.db), t);
+      BARRIER();
+    }
+    if (err) {
+      if (lead) {
+        atomicCAS(&ctl->err, 0, err);
+        p.brec[b].err = err;
+      }
+      return;
+    }
+    if (p.layout == 1) finish_vertex_major<WORDS>(p, gb, depth, n_b, t);
+    else finish_source_major<WORDS>(p, gb, depth, n_b, k0, dsmem, t);
+    if (lead) {
+      BatchRec r;
+      r.levels = level;
+      r.max_level = max_level;
+      r.td = td;
+      r.bu = bu;
+      r.teps = teps;
+      r.err = 0;
+      r.pad = 0;
+      p.brec[b] = r;
+    }
+    BARRIER();
+  }
+#undef BARRIER
+}
+
+// ---- plain schedule: one kernel per phase, the whole grid is the team ----
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_seed(Params p, int b) {
+  const Team t = make_team(blockIdx.x, gridDim.x);
+  const long long k0 = (long long)b * p.C;
+  const int n_b = (int)min((long long)p.C, p.n_total - k0);
+  seed_phase<WORDS>(p, p.groups[0], p.src + k0, n_b, t);
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_inspect(Params p, GroupBufs gb, int b, int level) {
+  const Team t = make_team(blockIdx.x, gridDim.x);
+  const long long k0 = (long long)b * p.C;
+  const int n_b = (int)min((long long)p.C, p.n_total - k0);
+  inspect_phase<WORDS>(p, gb, &gb.ctl->par[level & 1], batch_depth(p, gb, b), n_b, level,
+                       level <= depth_limit(p.db), t);
+}
+
+__global__ void __launch_bounds__(512) k_qbuild(Params p, GroupBufs gb, int level) {
+  const Team t = make_team(blockIdx.x, gridDim.x);
+  qbuild_phase(p, gb, gb.ctl->qc[level & 1], t);
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_td(Params p, GroupBufs gb, int level) {
+  const Team t = make_team(blockIdx.x, gridDim.x);
+  td_phase<WORDS>(p, gb, gb.ctl->qc[level & 1], t);
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_bu(Params p, GroupBufs gb, int level) {
+  const Team t = make_team(blockIdx.x, gridDim.x);
+  bu_phase<WORDS>(p, gb, gb.ctl->par[(level - 1) & 1].fmask, t);
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_finish(Params p, GroupBufs gb, int b) {
+  extern __shared__ __align__(16) uint8_t dsmem[];
+  const Team t = make_team(blockIdx.x, gridDim.x);
+  const long long k0 = (long long)b * p.C;
+  const int n_b = (int)min((long long)p.C, p.n_total - k0);
+  uint8_t* depth = batch_depth(p, gb, b);
+  if (p.layout == 1) finish_vertex_major<WORDS>(p, gb, depth, n_b, t);
+  else finish_source_major<WORDS>(p, gb, depth, n_b, k0, dsmem, t);
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+#define CU(call)                                       \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) {                           \
+      last_cuda_error() = e_;                          \
+      return e_ == cudaErrorMemoryAllocation ? IBFS_ERR_OOM : IBFS_ERR_CUDA; \
+    }                                                  \
+  } while (0)
+
+static cudaError_t& last_cuda_error() {
+  static thread_local cudaError_t e = cudaSuccess;
+  return e;
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ibfs_status ensure(size_t want) {
+    if (want <= bytes && p) return IBFS_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(want, 256));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      last_cuda_error() = e;
+      return IBFS_ERR_OOM;
+    }
+    bytes = std::max<size_t>(want, 256);
+    return IBFS_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct PinBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ibfs_status ensure(size_t want) {
+    if (want <= bytes && p) return IBFS_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    if (cudaMallocHost(&p, std::max<size_t>(want, 256)) != cudaSuccess) {
+      p = nullptr;
+      return IBFS_ERR_OOM;
+    }
+    bytes = std::max<size_t>(want, 256);
+    return IBFS_OK;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct GroupMem {
+  DevBuf last, curr, chg, qs, qm, ql, ctl, stage;
+  void release() {
+    last.release(); curr.release(); chg.release(); qs.release();
+    qm.release(); ql.release(); ctl.release(); stage.release();
+  }
+};
+
+struct GraphCache {
+  cudaGraphExec_t exec = nullptr;
+  std::string key;
+  void release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    key.clear();
+  }
+};
+
+}  // namespace ibfs
+
+using namespace ibfs;
+
+struct ibfs_graph {
+  int device = 0;
+  int sms = 0;
+  int64_t V = 0, E = 0, max_deg = 0;
+  HostCsr h;
+  DevBuf beg, col;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // workspace
+  std::vector<GroupMem> groups;
+  DevBuf d_groups, d_src, d_outrow, d_brec, d_lrec, d_out;
+  PinBuf h_src, h_outrow, h_brec, h_lrec, h_par;
+  GraphCache gcache;
+  std::mutex mu;
+};
+
+namespace ibfs {
+
+static const int kLrecCap = 1024;
+
+static int words_for(int width) { return width / 32; }
+
+static ibfs_status check_opts(const ibfs_opts* o) {
+  if (o->width != 32 && o->width != 64 && o->width != 128 && o->width != 256)
+    return IBFS_ERR_INVALID_ARG;
+  if (o->concurrent < 0 || o->concurrent > o->width) return IBFS_ERR_INVALID_ARG;
+  if (o->mode != IBFS_MODE_PLAIN && o->mode != IBFS_MODE_PERSISTENT) return IBFS_ERR_INVALID_ARG;
+  if (o->depth_bytes != 0 && o->depth_bytes != 1 && o->depth_bytes != 2) return IBFS_ERR_INVALID_ARG;
+  if (o->threads != 0 && o->threads != 128 && o->threads != 256 && o->threads != 512)
+    return IBFS_ERR_INVALID_ARG;
+  if (o->alpha <= 0 || o->beta <= 0) return IBFS_ERR_INVALID_ARG;
+  if (o->sml_shed < 1 || o->lrg_shed < o->sml_shed - 1) return IBFS_ERR_INVALID_ARG;
+  if (o->groups < 0 || o->ctas_per_sm < 0 || o->timeout_ms < 0 || o->max_levels < 0)
+    return IBFS_ERR_INVALID_ARG;
+  return IBFS_OK;
+}
+
+// Per-group workspace bytes for (V, W, C, db).
+static size_t group_bytes(int64_t V, int64_t E, int words, int C, int db, int lrg, int chunk,
+                          bool stage) {
+  const size_t vpad = (size_t)((V + 31) & ~31LL);
+  const size_t nchg = (size_t)(((V + 31) / 32 + 3) & ~3LL);
+  const size_t capl = (size_t)(E / std::max(chunk, 1) + std::min<int64_t>(V, E / std::max(lrg, 1)) + 16);
+  size_t b = 2 * vpad * words * 4 + nchg * 4 + 2 * (size_t)V * 4 + capl * 8 + sizeof(Ctl);
+  if (stage) b += (size_t)V * C * db;
+  return b;
+}
+
+template <int WORDS>
+static const void* persistent_fn() { return (const void*)persistent_kernel<WORDS>; }
+
+static const void* persistent_for(int words) {
+  switch (words) {
+    case 1: return persistent_fn<1>();
+    case 2: return persistent_fn<2>();
+    case 4: return persistent_fn<4>();
+    default: return persistent_fn<8>();
+  }
+}
+
+template <int WORDS>
+static cudaError_t launch_plain_level(const Params& p, const GroupBufs& gb, int grid, int threads,
+                                      int level, int dir, cudaStream_t s) {
+  if (dir == kDirTD) {
+    k_qbuild<<<grid, threads, 0, s>>>(p, gb, level);
+    k_td<WORDS><<<grid, threads, 0, s>>>(p, gb, level);
+  } else {
+    k_bu<WORDS><<<grid, threads, 0, s>>>(p, gb, level);
+  }
+  return cudaGetLastError();
+}
+
+template <int WORDS>
+static cudaError_t launch_plain_inspect(const Params& p, const GroupBufs& gb, int grid, int threads,
+                                        int b, int level, cudaStream_t s) {
+  k_inspect<WORDS><<<grid, threads, 0, s>>>(p, gb, b, level);
+  return cudaGetLastError();
+}
+
+template <int WORDS>
+static cudaError_t launch_plain_seed(const Params& p, int grid, int threads, int b, cudaStream_t s) {
+  k_seed<WORDS><<<grid, threads, 0, s>>>(p, b);
+  return cudaGetLastError();
+}
+
+template <int WORDS>
+static cudaError_t launch_plain_finish(const Params& p, const GroupBufs& gb, int grid, int threads,
+                                       int b, size_t smem, cudaStream_t s) {
+  k_finish<WORDS><<<grid, threads, smem, s>>>(p, gb, b);
+  return cudaGetLastError();
+}
+
+#define DISPATCH_WORDS(words, fn, ...)                  \
+  ((words) == 1   ? fn<1>(__VA_ARGS__)                  \
+   : (words) == 2 ? fn<2>(__VA_ARGS__)                  \
+   : (words) == 4 ? fn<4>(__VA_ARGS__)                  \
+                  : fn<8>(__VA_ARGS__))
+
+template <int WORDS>
+static cudaError_t set_smem_attrs(size_t smem) {
+  cudaError_t e = cudaFuncSetAttribute(persistent_kernel<WORDS>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_finish<WORDS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem);
+}
+
+struct RunPlan {
+  int words, C, nbatches, G, cpg, threads, grid, db;
+  size_t smem;
+  bool host_out;
+};
+
+// Allocate / reuse the workspace for G groups.
+static ibfs_status ensure_workspace(ibfs_graph* g, const RunPlan& rp, const ibfs_opts& o,
+                                    int layout) {
+  const bool stage = layout == IBFS_LAYOUT_SOURCE_MAJOR;
+  const size_t vpad = (size_t)((g->V + 31) & ~31LL);
+  const size_t nchg = (size_t)(((g->V + 31) / 32 + 3) & ~3LL);
+  const int chunk = rp.threads * 4;
+  const size_t capl = (size_t)(g->E / chunk + std::min<int64_t>(g->V, g->E / std::max(o.lrg_shed, 1)) + 16);
+  if ((int)g->groups.size() < rp.G) g->groups.resize(rp.G);
+  for (int i = 0; i < rp.G; i++) {
+    GroupMem& m = g->groups[i];
+    ibfs_status s;
+    if ((s = m.last.ensure(vpad * rp.words * 4)) != IBFS_OK) return s;
+    if ((s = m.curr.ensure(vpad * rp.words * 4)) != IBFS_OK) return s;
+    if ((s = m.chg.ensure(nchg * 4)) != IBFS_OK) return s;
+    if ((s = m.qs.ensure((size_t)g->V * 4)) != IBFS_OK) return s;
+    if ((s = m.qm.ensure((size_t)g->V * 4)) != IBFS_OK) return s;
+    if ((s = m.ql.ensure(capl * 8)) != IBFS_OK) return s;
+    if ((s = m.ctl.ensure(sizeof(Ctl))) != IBFS_OK) return s;
+    if (stage && (s = m.stage.ensure((size_t)g->V * rp.C * rp.db)) != IBFS_OK) return s;
+  }
+  return IBFS_OK;
+}
+
+static std::string make_key(const ibfs_graph* g, const int32_t* src, int64_t n, const ibfs_opts& o,
+                            void* out, int layout, uint32_t flags, const RunPlan& rp) {
+  std::string k;
+  k.append(reinterpret_cast<const char*>(&o), sizeof(o));
+  k.append(reinterpret_cast<const char*>(&rp), sizeof(rp));
+  k.append(reinterpret_cast<const char*>(&out), sizeof(out));
+  k.append(reinterpret_cast<const char*>(&layout), sizeof(layout));
+  k.append(reinterpret_cast<const char*>(&flags), sizeof(flags));
+  k.append(reinterpret_cast<const char*>(&n), sizeof(n));
+  k.append(reinterpret_cast<const char*>(&g->stream), sizeof(g->stream));
+  if (!(flags & IBFS_OUT_DEVICE)) k.append(reinterpret_cast<const char*>(src), sizeof(int32_t) * n);
+  return k;
+}
+
+}  // namespace ibfs
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" const char* ibfs_strerror(ibfs_status s) {
+  switch (s) {
+    case IBFS_OK: return "ok";
+    case IBFS_ERR_IO: return "i/o error (file missing, unreadable or short)";
+    case IBFS_ERR_FORMAT: return "malformed CSR input";
+    case IBFS_ERR_RANGE: return "value out of range (vertex id, edge count or BFS level)";
+    case IBFS_ERR_OOM: return "out of memory";
+    case IBFS_ERR_CUDA: return "CUDA error";
+    case IBFS_ERR_TIMEOUT: return "a bounded device wait timed out";
+    case IBFS_ERR_INVALID_ARG: return "invalid argument";
+    case IBFS_ERR_UNSUPPORTED: return "unsupported option combination";
+    case IBFS_ERR_BUSY: return "admission refused: server at capacity";
+    case IBFS_ERR_NOT_FOUND: return "unknown query id";
+  }
+  return "unknown status";
+}
+
+extern "C" const char* ibfs_version(void) { return "ibfs-b200 0.1 (sm_100a)"; }
+
+extern "C" void ibfs_opts_default(ibfs_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->width = 128;
+  o->concurrent = 0;
+  o->switch_level = -1;
+  o->alpha = 14.0f;
+  o->beta = 24.0f;
+  o->sml_shed = 32;
+  o->lrg_shed = 512;
+  o->mode = IBFS_MODE_PERSISTENT;
+  o->groupby = 0;
+  o->depth_bytes = 0;
+  o->groups = 0;
+  o->threads = 0;
+  o->ctas_per_sm = 0;
+  o->use_graph = 0;
+  o->timeout_ms = 0;
+  o->max_levels = 0;
+  o->debug_withhold = 0;
+}
+
+static ibfs_status upload_graph(ibfs_graph* g) {
+  CU(cudaSetDevice(g->device));
+  int sms = 0;
+  CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+  g->sms = sms;
+  ibfs_status s;
+  if ((s = g->beg.ensure(sizeof(int64_t) * (size_t)(g->V + 1))) != IBFS_OK) return s;
+  if ((s = g->col.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(g->E, 1))) != IBFS_OK) return s;
+  CU(cudaStreamCreateWithFlags(&g->own_stream, cudaStreamNonBlocking));
+  g->stream = g->own_stream;
+  CU(cudaEventCreate(&g->ev0));
+  CU(cudaEventCreate(&g->ev1));
+  CU(cudaMemcpyAsync(g->beg.p, g->h.beg.data(), sizeof(int64_t) * (size_t)(g->V + 1),
+                     cudaMemcpyHostToDevice, g->stream));
+  if (g->E)
+    CU(cudaMemcpyAsync(g->col.p, g->h.col.data(), sizeof(int32_t) * (size_t)g->E,
+                       cudaMemcpyHostToDevice, g->stream));
+  CU(cudaStreamSynchronize(g->stream));
+  int64_t md = 0;
+  for (int64_t v = 0; v < g->V; v++) md = std::max(md, g->h.beg[v + 1] - g->h.beg[v]);
+  g->max_deg = md;
+  return IBFS_OK;
+}
+
+static void destroy_graph(ibfs_graph* g) {
+  if (!g) return;
+  cudaSetDevice(g->device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  g->gcache.release();
+  for (auto& m : g->groups) m.release();
+  g->beg.release();
+  g->col.release();
+  g->d_groups.release();
+  g->d_src.release();
+  g->d_outrow.release();
+  g->d_brec.release();
+  g->d_lrec.release();
+  g->d_out.release();
+  g->h_src.release();
+  g->h_outrow.release();
+  g->h_brec.release();
+  g->h_lrec.release();
+  g->h_par.release();
+  if (g->ev0) cudaEventDestroy(g->ev0);
+  if (g->ev1) cudaEventDestroy(g->ev1);
+  if (g->own_stream) cudaStreamDestroy(g->own_stream);
+  delete g;
+}
+
+extern "C" ibfs_status ibfs_graph_open(const char* beg_path, const char* csr_path, int device,
+                                       ibfs_graph** out) {
+  if (!beg_path || !csr_path || !out) return IBFS_ERR_INVALID_ARG;
+  *out = nullptr;
+  ibfs_graph* g = new (std::nothrow) ibfs_graph();
+  if (!g) return IBFS_ERR_OOM;
+  g->device = device;
+  ibfs_status s = load_csr_files(beg_path, csr_path, &g->h);
+  if (s == IBFS_OK) {
+    g->V = g->h.V;
+    g->E = g->h.E;
+    s = upload_graph(g);
+  }
+  if (s != IBFS_OK) {
+    destroy_graph(g);
+    return s;
+  }
+  *out = g;
+  return IBFS_OK;
+}
+
+extern "C" ibfs_status ibfs_graph_from_csr(const int64_t* beg_pos_host, const int32_t* col_host,
+                                           int64_t V, int64_t E, int device, ibfs_graph** out) {
+  if (!beg_pos_host || (!col_host && E > 0) || !out || V <= 0 || E < 0) return IBFS_ERR_INVALID_ARG;
+  *out = nullptr;
+  ibfs_status s = validate_csr(beg_pos_host, col_host, V, E);
+  if (s != IBFS_OK) return s;
+  ibfs_graph* g = new (std::nothrow) ibfs_graph();
+  if (!g) return IBFS_ERR_OOM;
+  g->device = device;
+  try {
+    g->h.V = V;
+    g->h.E = E;
+    g->h.beg.assign(beg_pos_host, beg_pos_host + V + 1);
+    g->h.col.assign(col_host, col_host + E);
+  } catch (const std::bad_alloc&) {
+    delete g;
+    return IBFS_ERR_OOM;
+  }
+  g->V = V;
+  g->E = E;
+  s = upload_graph(g);
+  if (s != IBFS_OK) {
+    destroy_graph(g);
+    return s;
+  }
+  *out = g;
+  return IBFS_OK;
+}
+
+extern "C" ibfs_status ibfs_graph_info(const ibfs_graph* g, int64_t* V, int64_t* E,
+                                       int64_t* max_degree) {
+  if (!g) return IBFS_ERR_INVALID_ARG;
+  if (V) *V = g->V;
+  if (E) *E = g->E;
+  if (max_degree) *max_degree = g->max_deg;
+  return IBFS_OK;
+}
+
+extern "C" ibfs_status ibfs_graph_device_csr(const ibfs_graph* g, const int64_t** beg,
+                                             const int32_t** col) {
+  if (!g) return IBFS_ERR_INVALID_ARG;
+  if (beg) *beg = g->beg.as<int64_t>();
+  if (col) *col = g->col.as<int32_t>();
+  return IBFS_OK;
+}
+
+extern "C" ibfs_status ibfs_graph_close(ibfs_graph* g) {
+  if (!g) return IBFS_ERR_INVALID_ARG;
+  destroy_graph(g);
+  return IBFS_OK;
+}
+
+extern "C" ibfs_status ibfs_set_stream(ibfs_graph* g, void* cuda_stream) {
+  if (!g) return IBFS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g->mu);
+  g->stream = cuda_stream ? (cudaStream_t)cuda_stream : g->own_stream;
+  g->gcache.release();
+  return IBFS_OK;
+}
+
+extern "C" ibfs_status ibfs_groupby(const ibfs_graph* g, const int32_t* src_host, int64_t n,
+                                    int32_t* out_host) {
+  if (!g || (!src_host && n > 0) || (!out_host && n > 0) || n < 0) return IBFS_ERR_INVALID_ARG;
+  for (int64_t i = 0; i < n; i++)
+    if (src_host[i] < 0 || src_host[i] >= g->V) return IBFS_ERR_RANGE;
+  groupby_host(g->h.beg.data(), g->h.col.data(), g->V, src_host, n, out_host);
+  return IBFS_OK;
+}
+
+extern "C" ibfs_status ibfs_teps(const ibfs_graph* g, const void* depth_host, int64_t n,
+                                 int32_t depth_bytes, int64_t* edges) {
+  if (!g || !depth_host || !edges || n < 0 || (depth_bytes != 1 && depth_bytes != 2))
+    return IBFS_ERR_INVALID_ARG;
+  int64_t total = 0;
+  const int64_t V = g->V;
+#pragma omp parallel for reduction(+ : total) schedule(static)
+  for (int64_t i = 0; i < n; i++) {
+    int64_t t = 0;
+    for (int64_t v = 0; v < V; v++) {
+      const bool reached = depth_bytes == 1
+                               ? ((const uint8_t*)depth_host)[i * V + v] != 0xFF
+                               : ((const uint16_t*)depth_host)[i * V + v] != 0xFFFF;
+      if (reached) t += g->h.beg[v + 1] - g->h.beg[v];
+    }
+    total += t;
+  }
+  *edges = total;
+  return IBFS_OK;
+}
+
+// Order sources (GroupBy or identity) and map each ordered position to the
+// caller's index.  Duplicated ids keep their order of appearance.
+static void order_sources(const ibfs_graph* g, const int32_t* src, int64_t n, bool groupby,
+                          std::vector<int32_t>* ord, std::vector<int32_t>* row) {
+  ord->assign(src, src + n);
+  row->resize((size_t)n);
+  if (!groupby) {
+    std::iota(row->begin(), row->end(), 0);
+    return;
+  }
+  groupby_host(g->h.beg.data(), g->h.col.data(), g->V, src, n, ord->data());
+  // map ids back to positions (stable for duplicates)
+  std::vector<std::pair<int32_t, int32_t>> pos((size_t)n);
+  for (int64_t i = 0; i < n; i++) pos[i] = {src[i], (int32_t)i};
+  std::sort(pos.begin(), pos.end());
+  std::vector<int64_t> used;
+  std::vector<std::pair<int32_t, int32_t>> ordk((size_t)n);
+  for (int64_t k = 0; k < n; k++) ordk[k] = {(*ord)[k], (int32_t)k};
+  std::stable_sort(ordk.begin(), ordk.end(),
+                   [](const std::pair<int32_t, int32_t>& a, const std::pair<int32_t, int32_t>& b) {
+                     return a.first < b.first;
+                   });
+  // both sorted by id; equal ids pair up in order of appearance / order
+  for (int64_t i = 0; i < n; i++) (*row)[ordk[i].second] = pos[i].second;
+}
+
+static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const ibfs_opts& o,
+                            int db, void* depth_out, int32_t layout, uint32_t flags,
+                            ibfs_stats* st, bool* range_hit);
+
+extern "C" ibfs_status ibfs_run(ibfs_graph* g, const int32_t* src_host, int64_t n,
+                                const ibfs_opts* opts, void* depth_out, int32_t layout,
+                                uint32_t flags, ibfs_stats* stats) {
+  if (!g || !src_host || n <= 0 || !depth_out) return IBFS_ERR_INVALID_ARG;
+  if (layout != IBFS_LAYOUT_SOURCE_MAJOR && layout != IBFS_LAYOUT_VERTEX_MAJOR)
+    return IBFS_ERR_INVALID_ARG;
+  ibfs_opts o;
+  if (opts) o = *opts;
+  else ibfs_opts_default(&o);
+  ibfs_status s = check_opts(&o);
+  if (s != IBFS_OK) return s;
+  for (int64_t i = 0; i < n; i++)
+    if (src_host[i] < 0 || src_host[i] >= g->V) return IBFS_ERR_RANGE;
+  std::lock_guard<std::mutex> lk(g->mu);
+  if (cudaSetDevice(g->device) != cudaSuccess) return IBFS_ERR_CUDA;
+  const auto t0 = std::chrono::steady_clock::now();
+  bool range_hit = false;
+  int db = o.depth_bytes == 0 ? 1 : o.depth_bytes;
+  s = run_once(g, src_host, n, o, db, depth_out, layout, flags, stats, &range_hit);
+  if (s == IBFS_ERR_RANGE && range_hit && o.depth_bytes == 0) {
+    db = 2;
+    s = run_once(g, src_host, n, o, db, depth_out, layout, flags, stats, &range_hit);
+  }
+  if (stats) {
+    stats->total_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return s;
+}
+
+static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const ibfs_opts& o,
+                            int db, void* depth_out, int32_t layout, uint32_t flags,
+                            ibfs_stats* st, bool* range_hit) {
+  *range_hit = false;
+  cudaStream_t s = g->stream;
+  RunPlan rp;
+  std::memset(&rp, 0, sizeof(rp));
+  rp.words = words_for(o.width);
+  rp.C = o.concurrent ? o.concurrent : o.width;
+  rp.nbatches = (int)((n + rp.C - 1) / rp.C);
+  rp.threads = o.threads ? o.threads : 512;
+  rp.db = db;
+  rp.host_out = !(flags & IBFS_OUT_DEVICE);
+  rp.smem = layout == IBFS_LAYOUT_SOURCE_MAJOR ? transpose_smem_bytes(rp.C, db, rp.words) : 0;
+  const bool persistent = o.mode == IBFS_MODE_PERSISTENT;
+  if (rp.smem > 0) CU(DISPATCH_WORDS(rp.words, set_smem_attrs, rp.smem));
+  // grid sizing
+  int occ = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, persistent_for(rp.words), rp.threads,
+                                                   rp.smem));
+  if (occ < 1) return IBFS_ERR_UNSUPPORTED;
+  int per_sm = o.ctas_per_sm ? std::min(o.ctas_per_sm, occ) : occ;
+  const int total_ctas = g->sms * per_sm;
+  if (persistent) {
+    int G = o.groups;
+    if (G == 0) {
+      // enough CTAs per group to sweep V with >= 8 words of 32 vertices per warp
+      const int64_t want = std::max<int64_t>(1, (g->V + 32LL * 8 * (rp.threads / 32) - 1) /
+                                                    (32LL * 8 * (rp.threads / 32)));
+      G = (int)std::max<int64_t>(1, std::min<int64_t>(rp.nbatches, total_ctas / std::min<int64_t>(want, total_ctas)));
+      // memory guard
+      size_t freeb = 0, totb = 0;
+      if (cudaMemGetInfo(&freeb, &totb) == cudaSuccess) {
+        const size_t per = group_bytes(g->V, g->E, rp.words, rp.C, db, o.lrg_shed, rp.threads * 4,
+                                       layout == IBFS_LAYOUT_SOURCE_MAJOR);
+        const size_t budget = (size_t)(freeb * 0.5);
+        G = (int)std::max<size_t>(1, std::min<size_t>((size_t)G, budget / std::max<size_t>(per, 1)));
+      }
+    }
+    G = std::max(1, std::min(G, std::min(rp.nbatches, total_ctas)));
+    rp.G = G;
+    rp.cpg = total_ctas / G;
+    rp.grid = rp.cpg * G;
+  } else {
+    rp.G = 1;
+    rp.cpg = total_ctas;
+    rp.grid = total_ctas;
+  }
+  ibfs_status es = ensure_workspace(g, rp, o, layout);
+  if (es != IBFS_OK) return es;
+  // ordered sources and their output rows
+  std::vector<int32_t> ord, row;
+  order_sources(g, src, n, o.groupby != 0, &ord, &row);
+  ibfs_status bs;
+  if ((bs = g->h_src.ensure(sizeof(int32_t) * n)) != IBFS_OK) return bs;
+  if ((bs = g->h_outrow.ensure(sizeof(int32_t) * n)) != IBFS_OK) return bs;
+  if ((bs = g->d_src.ensure(sizeof(int32_t) * n)) != IBFS_OK) return bs;
+  if ((bs = g->d_outrow.ensure(sizeof(int32_t) * n)) != IBFS_OK) return bs;
+  if ((bs = g->d_brec.ensure(sizeof(BatchRec) * rp.nbatches)) != IBFS_OK) return bs;
+  if ((bs = g->h_brec.ensure(sizeof(BatchRec) * rp.nbatches)) != IBFS_OK) return bs;
+  if ((bs = g->d_lrec.ensure(sizeof(LevelRec) * (size_t)rp.nbatches * kLrecCap)) != IBFS_OK) return bs;
+  if ((bs = g->h_lrec.ensure(sizeof(LevelRec) * (size_t)rp.nbatches * kLrecCap)) != IBFS_OK) return bs;
+  if ((bs = g->d_groups.ensure(sizeof(GroupBufs) * rp.G)) != IBFS_OK) return bs;
+  if ((bs = g->h_par.ensure(sizeof(Ctl) * rp.G + sizeof(GroupBufs) * rp.G)) != IBFS_OK) return bs;
+  const size_t out_bytes = (size_t)n * (size_t)g->V * db;
+  uint8_t* dout = nullptr;
+  if (rp.host_out) {
+    if ((bs = g->d_out.ensure(out_bytes)) != IBFS_OK) return bs;
+    dout = g->d_out.as<uint8_t>();
+  } else {
+    dout = reinterpret_cast<uint8_t*>(depth_out);
+  }
+  // In the vertex-major layout batch blocks are [V][C] even for the last,
+  // partial batch: the block of batch b starts at b*V*C.
+  if (layout == IBFS_LAYOUT_VERTEX_MAJOR && rp.nbatches * (size_t)rp.C > (size_t)n) {
+    // the last batch uses V*n_b bytes of its block; the caller buffer holds
+    // exactly n*V*db bytes, which covers every block start.
+  }
+  std::memcpy(g->h_src.p, ord.data(), sizeof(int32_t) * n);
+  std::memcpy(g->h_outrow.p, row.data(), sizeof(int32_t) * n);
+  GroupBufs* hgb = reinterpret_cast<GroupBufs*>(g->h_par.as<uint8_t>() + sizeof(Ctl) * rp.G);
+  for (int i = 0; i < rp.G; i++) {
+    GroupMem& m = g->groups[i];
+    hgb[i].last = m.last.as<uint32_t>();
+    hgb[i].curr = m.curr.as<uint32_t>();
+    hgb[i].chg = m.chg.as<uint32_t>();
+    hgb[i].qs = m.qs.as<int32_t>();
+    hgb[i].qm = m.qm.as<int32_t>();
+    hgb[i].ql = m.ql.as<int2>();
+    hgb[i].ctl = m.ctl.as<Ctl>();
+    hgb[i].stage = layout == IBFS_LAYOUT_SOURCE_MAJOR ? m.stage.as<uint8_t>() : nullptr;
+  }
+  Params p;
+  std::memset(&p, 0, sizeof(p));
+  p.beg = g->beg.as<int64_t>();
+  p.col = g->col.as<int32_t>();
+  p.V = g->V;
+  p.E = g->E;
+  p.nchg = (g->V + 31) / 32;
+  p.src = g->d_src.as<int32_t>();
+  p.out_row = g->d_outrow.as<int32_t>();
+  p.n_total = n;
+  p.C = rp.C;
+  p.nbatches = rp.nbatches;
+  p.G = rp.G;
+  p.cpg = rp.cpg;
+  p.db = db;
+  p.layout = layout;
+  p.out = dout;
+  p.sml = o.sml_shed;
+  p.lrg = o.lrg_shed;
+  p.chunk = rp.threads * 4;
+  p.but = 32;
+  p.switch_level = o.switch_level;
+  p.alpha = o.alpha;
+  p.beta = o.beta;
+  p.max_levels = o.max_levels ? o.max_levels : 65534;
+  p.timeout_ns = (unsigned long long)(o.timeout_ms ? o.timeout_ms : 10000) * 1000000ull;
+  p.withhold = o.debug_withhold;
+  p.groups = g->d_groups.as<GroupBufs>();
+  p.brec = g->d_brec.as<BatchRec>();
+  p.lrec = g->d_lrec.as<LevelRec>();
+  p.lrec_cap = kLrecCap;
+  p.vec_out = (g->V % 4 == 0) && ((reinterpret_cast<uintptr_t>(dout) & 7) == 0);
+
+  int64_t launches = 0;
+  const bool use_graph = persistent && o.use_graph && !o.debug_withhold;
+  std::string key;
+  bool replay = false;
+  if (use_graph) {
+    key = make_key(g, src, n, o, depth_out, layout, flags, rp);
+    replay = g->gcache.exec && g->gcache.key == key;
+  }
+
+  auto enqueue = [&](cudaStream_t cs, bool capturing) -> ibfs_status {
+    CU(cudaMemcpyAsync(g->d_src.p, g->h_src.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, cs));
+    CU(cudaMemcpyAsync(g->d_outrow.p, g->h_outrow.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, cs));
+    CU(cudaMemcpyAsync(g->d_groups.p, hgb, sizeof(GroupBufs) * rp.G, cudaMemcpyHostToDevice, cs));
+    for (int i = 0; i < rp.G; i++) CU(cudaMemsetAsync(hgb[i].ctl, 0, sizeof(Ctl), cs));
+    CU(cudaMemsetAsync(g->d_brec.p, 0, sizeof(BatchRec) * rp.nbatches, cs));
+    CU(cudaEventRecord(g->ev0, cs));
+    if (persistent) {
+      cudaLaunchConfig_t cfg;
+      std::memset(&cfg, 0, sizeof(cfg));
+      cfg.gridDim = dim3((unsigned)rp.grid);
+      cfg.blockDim = dim3((unsigned)rp.threads);
+      cfg.dynamicSmemBytes = rp.smem;
+      cfg.stream = cs;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeCooperative;
+      attr[0].val.cooperative = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      void* args[] = {&p};
+      CU(cudaLaunchKernelExC(&cfg, persistent_for(rp.words), args));
+      launches += 1;
+    }
+    CU(cudaEventRecord(g->ev1, cs));
+    if (rp.host_out) {
+      if (layout == IBFS_LAYOUT_SOURCE_MAJOR || true) {
+        CU(cudaMemcpyAsync(depth_out, dout, out_bytes, cudaMemcpyDeviceToHost, cs));
+      }
+    }
+    (void)capturing;
+    return IBFS_OK;
+  };
+
+  if (persistent) {
+    if (use_graph) {
+      if (!replay) {
+        g->gcache.release();
+        cudaGraph_t graph = nullptr;
+        CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        ibfs_status es2 = enqueue(s, true);
+        cudaGraph_t got = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(s, &got);
+        graph = got;
+        if (es2 != IBFS_OK) {
+          if (graph) cudaGraphDestroy(graph);
+          return es2;
+        }
+        if (ce != cudaSuccess) {
+          last_cuda_error() = ce;
+          if (graph) cudaGraphDestroy(graph);
+          return IBFS_ERR_CUDA;
+        }
+        cudaGraphExec_t exec = nullptr;
+        cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) {
+          last_cuda_error() = ie;
+          return IBFS_ERR_CUDA;
+        }
+        g->gcache.exec = exec;
+        g->gcache.key = key;
+      } else {
+        launches = 1;
+      }
+      CU(cudaGraphLaunch(g->gcache.exec, s));
+    } else {
+      ibfs_status es2 = enqueue(s, false);
+      if (es2 != IBFS_OK) return es2;
+    }
+  } else {
+    // ---- plain schedule -------------------------------------------------
+    CU(cudaMemcpyAsync(g->d_src.p, g->h_src.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(g->d_outrow.p, g->h_outrow.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(g->d_groups.p, hgb, sizeof(GroupBufs) * 1, cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(g->d_brec.p, 0, sizeof(BatchRec) * rp.nbatches, s));
+    CU(cudaEventRecord(g->ev0, s));
+    const GroupBufs gb = hgb[0];
+    const int grid = rp.grid, thr = rp.threads;
+    Par* hpar = reinterpret_cast<Par*>(g->h_par.p);
+    BatchRec* hbr = g->h_brec.as<BatchRec>();
+    LevelRec* hlr = g->h_lrec.as<LevelRec>();
+    const size_t vpad = (size_t)((g->V + 31) & ~31LL);
+    const size_t nchg = (size_t)(((g->V + 31) / 32 + 3) & ~3LL);
+    for (int b = 0; b < rp.nbatches; b++) {
+      CU(cudaMemsetAsync(gb.last, 0, vpad * rp.words * 4, s));
+      CU(cudaMemsetAsync(gb.curr, 0, vpad * rp.words * 4, s));
+      CU(cudaMemsetAsync(gb.chg, 0, nchg * 4, s));
+      CU(cudaMemsetAsync(gb.ctl, 0, sizeof(Ctl), s));
+      CU(DISPATCH_WORDS(rp.words, launch_plain_seed, p, grid, thr, b, s));
+      CU(DISPATCH_WORDS(rp.words, launch_plain_inspect, p, gb, grid, thr, b, 0, s));
+      launches += 2;
+      int level = 0, cur_dir = kDirTD, max_level = 0, td = 0, bu = 0, err = 0;
+      unsigned long long m_u = (unsigned long long)g->E, teps = 0;
+      while (true) {
+        CU(cudaMemcpyAsync(hpar, &gb.ctl->par[level & 1], sizeof(Par), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        const Par pr = *hpar;
+        teps += pr.teps;
+        m_u = m_u > pr.cdeg ? m_u - pr.cdeg : 0ull;
+        int stop = 0;
+        if (pr.range_err) { stop = 1; err = 3; }
+        else if (pr.changed == 0) stop = 1;
+        else if (level + 1 > p.max_levels) { stop = 1; err = 3; }
+        if (pr.changed && !pr.range_err) max_level = level;
+        const int nd = choose_dir(level + 1, cur_dir, p.switch_level, p.alpha, p.beta, pr.changed,
+                                  pr.mf, m_u, p.V);
+        if (level < kLrecCap) {
+          LevelRec& r = hlr[(size_t)b * kLrecCap + level];
+          r.batch = b; r.level = level; r.dir = level == 0 ? -1 : cur_dir; r.pad = 0;
+          r.frontier = (long long)pr.changed; r.frontier_edges = (long long)pr.mf;
+        }
+        if (stop) break;
+        cur_dir = nd;
+        level++;
+        CU(cudaMemsetAsync(&gb.ctl->par[level & 1], 0, sizeof(Par), s));
+        CU(cudaMemsetAsync(&gb.ctl->qc[level & 1][0], 0, sizeof(int32_t) * 4, s));
+        CU(DISPATCH_WORDS(rp.words, launch_plain_level, p, gb, grid, thr, level, cur_dir, s));
+        launches += cur_dir == kDirTD ? 2 : 1;
+        if (cur_dir == kDirTD) td++; else bu++;
+        CU(DISPATCH_WORDS(rp.words, launch_plain_inspect, p, gb, grid, thr, b, level, s));
+        launches += 1;
+      }
+      BatchRec& r = hbr[b];
+      r.levels = level; r.max_level = max_level; r.td = td; r.bu = bu; r.teps = teps; r.err = err;
+      if (err) {
+        *range_hit = err == 3;
+        return (ibfs_status)err;
+      }
+      CU(DISPATCH_WORDS(rp.words, launch_plain_finish, p, gb, grid, thr, b, rp.smem, s));
+      launches += 1;
+    }
+    CU(cudaEventRecord(g->ev1, s));
+    if (rp.host_out) CU(cudaMemcpyAsync(depth_out, dout, out_bytes, cudaMemcpyDeviceToHost, s));
+  }
+  CU(cudaStreamSynchronize(s));
+  // collect results
+  if (persistent) {
+    CU(cudaMemcpy(g->h_brec.p, g->d_brec.p, sizeof(BatchRec) * rp.nbatches, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(g->h_lrec.p, g->d_lrec.p, sizeof(LevelRec) * (size_t)rp.nbatches * kLrecCap,
+                  cudaMemcpyDeviceToHost));
+    int gerr = 0;
+    for (int i = 0; i < rp.G; i++) {
+      int e = 0;
+      CU(cudaMemcpy(&e, &hgb[i].ctl->err, sizeof(int), cudaMemcpyDeviceToHost));
+      if (e && !gerr) gerr = e;
+    }
+    if (gerr) {
+      *range_hit = gerr == 3;
+      return (ibfs_status)gerr;
+    }
+  }
+  const BatchRec* br = g->h_brec.as<BatchRec>();
+  if (st) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    st->n_sources = n;
+    st->n_batches = rp.nbatches;
+    st->depth_bytes = db;
+    st->width = o.width;
+    st->groups = rp.G;
+    st->max_level = 0;
+    st->levels_total = st->td_levels = st->bu_levels = 0;
+    st->traversed_edges = 0;
+    for (int b = 0; b < rp.nbatches; b++) {
+      st->max_level = std::max(st->max_level, br[b].max_level);
+      st->levels_total += br[b].levels;
+      st->td_levels += br[b].td;
+      st->bu_levels += br[b].bu;
+      st->traversed_edges += (int64_t)br[b].teps;
+    }
+    st->gpu_launches = launches;
+    st->device_ms = ms;
+    st->levels_len = 0;
+    if (st->levels && st->levels_cap > 0) {
+      const LevelRec* lr = g->h_lrec.as<LevelRec>();
+      int k = 0;
+      for (int b = 0; b < rp.nbatches && k < st->levels_cap; b++)
+        for (int l = 0; l <= std::min(br[b].levels, kLrecCap - 1) && k < st->levels_cap; l++) {
+          const LevelRec& r = lr[(size_t)b * kLrecCap + l];
+          ibfs_level_rec& o2 = st->levels[k++];
+          o2.batch = r.batch; o2.level = r.level; o2.dir = r.dir; o2.pad = 0;
+          o2.frontier = r.frontier; o2.frontier_edges = r.frontier_edges;
+        }
+      st->levels_len = k;
+    }
+  }
+  return IBFS_OK;
+}

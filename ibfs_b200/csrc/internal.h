@@ -1,0 +1,42 @@
+// internal.h -- declarations shared by the host C++ and CUDA sources of libibfs.
+#pragma once
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+
+#include "../../include/ibfs.h"
+
+namespace ibfs {
+
+// Counter-based 64-bit hash (splitmix64 finaliser, Steele/Lea/Flood 2014):
+// every generator draws value i of stream `stream` as rnd(seed, stream, i),
+// so generation is parallel and independent of the thread count.
+static inline uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+static inline uint64_t rnd(uint64_t seed, uint64_t stream, uint64_t i) {
+  return mix64(mix64(seed ^ (stream * 0xD1B54A32D192ED03ull)) + i);
+}
+
+// Host CSR (int64 offsets, int32 column ids).
+struct HostCsr {
+  int64_t V = 0, E = 0;
+  std::vector<int64_t> beg;
+  std::vector<int32_t> col;
+};
+
+// Symmetrise, drop self-loops, sort and dedupe every adjacency list.
+ibfs_status build_csr(const int32_t* u, const int32_t* v, int64_t m, int64_t V,
+                      HostCsr* out);
+ibfs_status load_csr_files(const char* beg_path, const char* csr_path,
+                           HostCsr* out);
+ibfs_status validate_csr(const int64_t* beg, const int32_t* col, int64_t V,
+                         int64_t E);
+void groupby_host(const int64_t* beg, const int32_t* col, int64_t V,
+                  const int32_t* src, int64_t n, int32_t* out);
+
+}  // namespace ibfs

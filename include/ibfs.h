@@ -1,0 +1,208 @@
+/*
+ * ibfs.h -- C ABI of the B200 concurrent multi-source BFS (iBFS hot path).
+ *
+ * Every entry point takes plain pointers and sizes, returns an ibfs_status,
+ * never exits the process and never throws across the ABI.  Pointers named
+ * *_host are host memory; depth outputs may be host or device memory as
+ * flagged.  One handle is used by one host thread at a time; the server
+ * (ibfs_server_*) is thread-safe.
+ *
+ * Reference interfaces each entry point replaces (file:line in iBFS):
+ *   ibfs_graph_open        graph_reader::graph_reader      graph_reader.cuh:63-119
+ *                          (+ graph<>::alloc_array CSR upload allocator.cuh:3-80)
+ *   ibfs_graph_from_csr    graph<>::graph + alloc_array    graph.cuh:246-283, allocator.cuh:18-45
+ *   ibfs_graph_close       (none: the reference never frees, gpu_ibfs.cuh:100)
+ *   ibfs_groupby           GroupBy                         GroupBy.cuh:6-115
+ *   ibfs_run               graph<>::bfs_gpu_coalescing_mem bfs_gpu_opt.cuh:182-262
+ *                          -> ibfs()                       bfs_gpu_opt.cuh:39-177
+ *   ibfs_read_sources      read_src_v                      graph.cuh:99-133
+ *   ibfs_teps              report                          validate.h:59-76
+ *   ibfs_strerror          H_ERR / HandleError             comm.h:5-16
+ *   ibfs_server_*          (none: the reference runs fixed source lists)
+ */
+#ifndef IBFS_H
+#define IBFS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ibfs_status {
+    IBFS_OK = 0,
+    IBFS_ERR_IO = 1,          /* file missing / unreadable / short read      */
+    IBFS_ERR_FORMAT = 2,      /* CSR files inconsistent                       */
+    IBFS_ERR_RANGE = 3,       /* ids or levels do not fit the chosen types    */
+    IBFS_ERR_OOM = 4,         /* host or device allocation failed             */
+    IBFS_ERR_CUDA = 5,        /* a CUDA call failed                           */
+    IBFS_ERR_TIMEOUT = 6,     /* a bounded device wait gave up                */
+    IBFS_ERR_INVALID_ARG = 7, /* bad argument                                 */
+    IBFS_ERR_UNSUPPORTED = 8, /* option combination not built                 */
+    IBFS_ERR_BUSY = 9,        /* admission refused (server full)              */
+    IBFS_ERR_NOT_FOUND = 10   /* unknown query id                             */
+} ibfs_status;
+
+/* Execution schedules of one run (all give identical depths). */
+typedef enum ibfs_mode {
+    /* host-driven level loop, one launch per phase, host sync per level:
+       the reference's structure (bfs_gpu_opt.cuh:99-166) on sm_100a */
+    IBFS_MODE_PLAIN = 0,
+    /* one persistent level-synchronous launch for all levels of all batches */
+    IBFS_MODE_PERSISTENT = 1
+} ibfs_mode;
+
+/* Layout of the depth output of ibfs_run. */
+typedef enum ibfs_layout {
+    /* depth[i*V + v] = level of v from src[i], sources in the caller's order */
+    IBFS_LAYOUT_SOURCE_MAJOR = 0,
+    /* per batch b (after GroupBy), rows of that batch's sources:
+       depth[b*V*C + v*nb + j] where C = concurrent and nb = sources in b;
+       the reference's depth_merge layout (inspector.cuh:48) */
+    IBFS_LAYOUT_VERTEX_MAJOR = 1
+} ibfs_layout;
+
+/* Flags of ibfs_run. */
+#define IBFS_OUT_DEVICE 1u /* depth_out is a device pointer on the graph's GPU */
+
+typedef struct ibfs_graph ibfs_graph;
+
+typedef struct ibfs_opts {
+    int32_t width;         /* status bits per vertex: 32, 64, 128 or 256          */
+    int32_t concurrent;    /* sources per batch, 1..width (0: width)              */
+    int32_t switch_level;  /* >= 0: fixed switch as the reference's CLI argument:
+                              top-down while level <= switch_level, bottom-up after;
+                              -1: alpha/beta switching                            */
+    float alpha;           /* TD->BU when frontier_edges > unexplored_edges/alpha */
+    float beta;            /* BU->TD when frontier_vertices < V/beta              */
+    int32_t sml_shed;      /* degree < sml_shed: one thread per vertex (default 32) */
+    int32_t lrg_shed;      /* degree > lrg_shed: CTA chunks (default 512)         */
+    int32_t mode;          /* ibfs_mode                                           */
+    int32_t groupby;       /* 1: reorder sources with GroupBy before batching     */
+    int32_t depth_bytes;   /* 1 (INFTY 255) or 2 (INFTY 65535); 0: 1, widened to 2
+                              automatically when a level exceeds 254              */
+    int32_t groups;        /* batches run concurrently in one launch (0: auto)    */
+    int32_t threads;       /* threads per CTA (0: 512)                            */
+    int32_t ctas_per_sm;   /* persistent grid = SMs * ctas_per_sm (0: auto)       */
+    int32_t use_graph;     /* 1: capture the run in a CUDA graph, replay on reuse */
+    int32_t timeout_ms;    /* budget of every bounded device wait (0: 10000)      */
+    int32_t max_levels;    /* abort with IBFS_ERR_RANGE beyond this (0: 65534)    */
+    int32_t debug_withhold;/* test hook: CTA 0 never arrives at its first grid
+                              barrier, so every wait runs out (IBFS_ERR_TIMEOUT)  */
+    int32_t reserved[7];
+} ibfs_opts;
+
+typedef struct ibfs_level_rec {
+    int32_t batch;         /* batch index                                         */
+    int32_t level;         /* level expanded                                      */
+    int32_t dir;           /* 0 top-down, 1 bottom-up                             */
+    int32_t pad;
+    int64_t frontier;      /* vertices whose status changed at this level         */
+    int64_t frontier_edges;/* sum of their degrees                                */
+} ibfs_level_rec;
+
+typedef struct ibfs_stats {
+    int64_t n_sources;
+    int64_t n_batches;
+    int32_t max_level;      /* deepest BFS level over all sources                 */
+    int32_t depth_bytes;    /* depth type actually used                           */
+    int32_t width;          /* status width actually used                         */
+    int32_t groups;         /* concurrent batches per launch actually used        */
+    int64_t levels_total;   /* sum over batches of levels expanded                */
+    int64_t td_levels;
+    int64_t bu_levels;
+    int64_t traversed_edges;/* sum_s sum_{v reached from s} deg(v)                */
+    int64_t gpu_launches;   /* kernels launched by this run                       */
+    double device_ms;       /* device time of the traversal (CUDA events)         */
+    double total_ms;        /* wall time of the call incl. transfers              */
+    ibfs_level_rec *levels; /* optional caller array for per-level records        */
+    int32_t levels_cap;     /* its capacity                                       */
+    int32_t levels_len;     /* records written                                    */
+} ibfs_stats;
+
+/* ---- status ------------------------------------------------------------ */
+const char *ibfs_strerror(ibfs_status s);
+/* Library version string. */
+const char *ibfs_version(void);
+
+/* ---- graph ------------------------------------------------------------- */
+/* Load <beg_pos.bin> ((V+1) little-endian uint64, beg[V]=E) and <csr.bin>
+   (E uint64), validate, and upload to `device`. */
+ibfs_status ibfs_graph_open(const char *beg_path, const char *csr_path,
+                            int device, ibfs_graph **out);
+/* Same from host arrays (beg_pos int64[V+1], col int32[E]); data is copied. */
+ibfs_status ibfs_graph_from_csr(const int64_t *beg_pos_host,
+                                const int32_t *col_host, int64_t V,
+                                int64_t E, int device, ibfs_graph **out);
+ibfs_status ibfs_graph_info(const ibfs_graph *g, int64_t *V, int64_t *E,
+                            int64_t *max_degree);
+/* Device pointers of the resident CSR (beg int64[V+1], col int32[E]). */
+ibfs_status ibfs_graph_device_csr(const ibfs_graph *g, const int64_t **beg,
+                                  const int32_t **col);
+ibfs_status ibfs_graph_close(ibfs_graph *g);
+
+/* ---- sources ----------------------------------------------------------- */
+/* GroupBy reorder (host, exact restatement of GroupBy.cuh:19-84). */
+ibfs_status ibfs_groupby(const ibfs_graph *g, const int32_t *src_host,
+                         int64_t n, int32_t *out_host);
+/* read_src_v format: one decimal vertex id per line.  With ids == NULL only
+   *n is set; otherwise up to cap ids are written. */
+ibfs_status ibfs_read_sources(const char *path, int32_t *ids, int64_t cap,
+                              int64_t *n);
+ibfs_status ibfs_write_sources(const char *path, const int32_t *ids, int64_t n);
+
+/* ---- traversal --------------------------------------------------------- */
+void ibfs_opts_default(ibfs_opts *o);
+/* Concurrent BFS from n sources.  depth_out holds n*V*depth_bytes bytes in
+   `layout`; flags: IBFS_OUT_DEVICE.  stats may be NULL.  Replays the cached
+   CUDA graph when opts->use_graph is set and the call matches the last one. */
+ibfs_status ibfs_run(ibfs_graph *g, const int32_t *src_host, int64_t n,
+                     const ibfs_opts *opts, void *depth_out, int32_t layout,
+                     uint32_t flags, ibfs_stats *stats);
+/* Launch on a caller stream (cudaStream_t) instead of the handle's own. */
+ibfs_status ibfs_set_stream(ibfs_graph *g, void *cuda_stream);
+
+/* TEPS numerator on the host: sum over sources of deg(v) for reached v
+   (validate.h:59-76) of a source-major depth array. */
+ibfs_status ibfs_teps(const ibfs_graph *g, const void *depth_host, int64_t n,
+                      int32_t depth_bytes, int64_t *edges);
+
+/* Algorithmic bytes of one batch (the implementation-independent byte
+   model: sum over levels of min(top-down, bottom-up) bytes plus status init
+   and depth output), computed on the GPU from a device source-major depth
+   array of n sources. */
+ibfs_status ibfs_bytes_alg(ibfs_graph *g, const void *depth_dev, int64_t n,
+                           int32_t depth_bytes, int32_t width, int64_t *bytes);
+
+/* ---- synthetic inputs (seeded, deterministic, host) -------------------- */
+/* Each generator symmetrises, drops self-loops, dedupes and sorts every
+   adjacency list.  Arrays are malloc'ed by the library; free with ibfs_free. */
+ibfs_status ibfs_gen_rmat(int32_t scale, int32_t edge_factor, double a,
+                          double b, double c, uint64_t seed, int64_t **beg,
+                          int32_t **col, int64_t *V, int64_t *E);
+ibfs_status ibfs_gen_grid(int32_t rows, int32_t cols, double delete_frac,
+                          double shortcut_frac, uint64_t seed, int64_t **beg,
+                          int32_t **col, int64_t *V, int64_t *E);
+ibfs_status ibfs_gen_chung_lu(int64_t n, int64_t m, double gamma,
+                              double max_degree, uint64_t seed, int64_t **beg,
+                              int32_t **col, int64_t *V, int64_t *E);
+/* Build a CSR from an undirected edge list (same cleaning rules). */
+ibfs_status ibfs_csr_from_edges(const int32_t *src, const int32_t *dst,
+                                int64_t m, int64_t V, int64_t **beg,
+                                int32_t **col, int64_t *E);
+/* Write the reference's binary CSR pair (uint64 little-endian). */
+ibfs_status ibfs_write_csr(const char *beg_path, const char *csr_path,
+                           const int64_t *beg, const int32_t *col, int64_t V);
+/* Sample n distinct sources uniformly (seeded) among vertices with degree
+   > 0 (component < 0) or inside the largest connected component
+   (component >= 0). */
+ibfs_status ibfs_sample_sources(const int64_t *beg, const int32_t *col,
+                                int64_t V, int64_t n, uint64_t seed,
+                                int32_t component, int32_t *out);
+void ibfs_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IBFS_H */

@@ -1,0 +1,223 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Integer work, so the bar is bit-exact depths for every source and an exact
+traversed-edge count.  Covers every status width, both schedules, both output
+layouts, partial and multiple batches, several concurrent groups, GroupBy,
+the fixed and the alpha/beta direction switch, one- and two-byte depths, and
+the edge cases of the reference's inputs (isolated and duplicated sources,
+disconnected graphs, hubs, a long path).
+"""
+import numpy as np
+import pytest
+
+import ibfs_b200 as ib
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+WIDTHS = [32, 64, 128, 256]
+
+
+def _graph(kind: str):
+    if kind == "rmat10":
+        return ib.gen_rmat(10, 16, seed=11)
+    if kind == "rmat13":
+        return ib.gen_rmat(13, 16, seed=1)
+    if kind == "rmat15":
+        return ib.gen_rmat(15, 16, seed=2)
+    if kind == "grid":
+        return ib.gen_grid(64, 80, 0.05, 0.001, seed=4)
+    if kind == "chunglu":
+        return ib.gen_chung_lu(20000, 600000, 2.1, 3000.0, seed=5)
+    raise KeyError(kind)
+
+
+_CACHE = {}
+
+
+def graph(kind):
+    if kind not in _CACHE:
+        beg, col = _graph(kind)
+        _CACHE[kind] = (beg, col, ib.Graph.from_csr(beg, col))
+    return _CACHE[kind]
+
+
+def run_and_check(beg, col, g, src, layout=ib.LAYOUT_SOURCE_MAJOR, **kw):
+    res = g.run(src, layout=layout, **kw)
+    ref, _ = oracle.bfs_auto(beg, col, src)
+    got = res.depth
+    if layout == ib.LAYOUT_VERTEX_MAJOR:
+        C = kw.get("concurrent", 0) or kw.get("width", 128)
+        V = len(beg) - 1
+        order = g.groupby(src) if kw.get("groupby") else np.asarray(src, np.int32)
+        ref_o, _ = oracle.bfs_auto(beg, col, order)
+        parts = []
+        flat = got.reshape(-1)
+        for b0 in range(0, len(src), C):
+            nb = min(C, len(src) - b0)
+            blk = flat[b0 * V:(b0 + nb) * V].reshape(V, nb)
+            parts.append(blk.T)
+        got = np.concatenate(parts, axis=0)
+        ref = ref_o
+    assert got.dtype == ref.dtype, (got.dtype, ref.dtype)
+    assert got.shape == ref.shape
+    mism = np.argwhere(got != ref)
+    assert len(mism) == 0, f"{len(mism)} mismatches, first {mism[:5].tolist()}"
+    assert res.stats["traversed_edges"] == oracle.teps(beg, ref)
+    return res
+
+
+@pytest.mark.parametrize("width", WIDTHS)
+@pytest.mark.parametrize("mode", [ib.MODE_PLAIN, ib.MODE_PERSISTENT])
+def test_rmat_widths_modes(width, mode):
+    beg, col, g = graph("rmat13")
+    src = ib.sample_sources(beg, col, width, seed=1)
+    run_and_check(beg, col, g, src, width=width, mode=mode)
+
+
+@pytest.mark.parametrize("width", WIDTHS)
+def test_partial_and_multi_batch(width):
+    beg, col, g = graph("rmat10")
+    src = ib.sample_sources(beg, col, 2 * width + 7, seed=3)
+    run_and_check(beg, col, g, src, width=width, mode=ib.MODE_PERSISTENT)
+    run_and_check(beg, col, g, src[:5], width=width, mode=ib.MODE_PERSISTENT)
+
+
+@pytest.mark.parametrize("groups", [1, 2, 3, 5])
+def test_groups(groups):
+    beg, col, g = graph("rmat13")
+    src = ib.sample_sources(beg, col, 5 * 64, seed=7)
+    run_and_check(beg, col, g, src, width=64, mode=ib.MODE_PERSISTENT, groups=groups)
+
+
+@pytest.mark.parametrize("layout", [ib.LAYOUT_SOURCE_MAJOR, ib.LAYOUT_VERTEX_MAJOR])
+@pytest.mark.parametrize("mode", [ib.MODE_PLAIN, ib.MODE_PERSISTENT])
+def test_layouts(layout, mode):
+    beg, col, g = graph("rmat10")
+    src = ib.sample_sources(beg, col, 300, seed=5)
+    run_and_check(beg, col, g, src, layout=layout, width=128, mode=mode)
+    run_and_check(beg, col, g, src, layout=layout, width=128, mode=mode, groupby=1)
+
+
+@pytest.mark.parametrize("kind", ["grid", "chunglu", "rmat15"])
+def test_graph_families(kind):
+    beg, col, g = graph(kind)
+    src = ib.sample_sources(beg, col, 256, seed=9)
+    run_and_check(beg, col, g, src, width=128, mode=ib.MODE_PERSISTENT)
+    run_and_check(beg, col, g, src[:128], width=256, mode=ib.MODE_PLAIN)
+
+
+@pytest.mark.parametrize("sw", [0, 1, 2, 5, 1000])
+def test_fixed_switch_level(sw):
+    beg, col, g = graph("rmat13")
+    src = ib.sample_sources(beg, col, 128, seed=2)
+    res = run_and_check(beg, col, g, src, width=128, switch_level=sw, levels_cap=64)
+    dirs = [r["dir"] for r in res.levels if r["level"] > 0]
+    for r in res.levels:
+        if r["level"] > 0:
+            assert r["dir"] == (0 if r["level"] <= sw else 1)
+    assert dirs
+
+
+@pytest.mark.parametrize("alpha,beta", [(1e-6, 1e6), (1e9, 1e-9), (14.0, 24.0), (2.0, 100.0)])
+def test_alpha_beta(alpha, beta):
+    beg, col, g = graph("chunglu")
+    src = ib.sample_sources(beg, col, 200, seed=4)
+    run_and_check(beg, col, g, src, width=256, alpha=alpha, beta=beta)
+
+
+@pytest.mark.parametrize("thr", [(1, 1), (32, 512), (4, 64), (64, 64), (1000000, 1000000)])
+def test_degree_thresholds(thr):
+    beg, col, g = graph("rmat13")
+    src = ib.sample_sources(beg, col, 128, seed=8)
+    run_and_check(beg, col, g, src, width=128, sml_shed=thr[0], lrg_shed=thr[1],
+                  switch_level=1000)
+
+
+def test_edge_case_graph():
+    # two components, an isolated vertex, a hub, a self loop and duplicates in
+    # the edge list (cleaned by the CSR builder), a 3-vertex path
+    e = [(0, 1), (1, 2), (2, 3), (3, 0), (0, 0), (0, 1), (4, 5), (5, 6)]
+    e += [(7, i) for i in range(8, 40)]
+    u = np.array([a for a, _ in e], np.int32)
+    v = np.array([b for _, b in e], np.int32)
+    beg, col = ib.csr_from_edges(u, v, 41)  # vertex 40 isolated
+    g = ib.Graph.from_csr(beg, col)
+    src = np.array([0, 40, 4, 7, 7, 39, 2, 0], np.int32)  # isolated + duplicates
+    for w in WIDTHS:
+        for mode in (ib.MODE_PLAIN, ib.MODE_PERSISTENT):
+            run_and_check(beg, col, g, src, width=w, mode=mode)
+    g.close()
+
+
+def test_long_path_uint16_widening():
+    n = 700
+    u = np.arange(n - 1, dtype=np.int32)
+    beg, col = ib.csr_from_edges(u, u + 1, n)
+    g = ib.Graph.from_csr(beg, col)
+    src = np.array([0, n - 1, n // 2], np.int32)
+    for mode in (ib.MODE_PLAIN, ib.MODE_PERSISTENT):
+        res = run_and_check(beg, col, g, src, width=32, mode=mode)
+        assert res.depth.dtype == np.uint16
+        assert res.stats["max_level"] == n - 1
+        # explicit one-byte depth must refuse instead of wrapping (comm.h:43)
+        with pytest.raises(ib.IbfsError) as ei:
+            g.run(src, width=32, mode=mode, depth_bytes=1)
+        assert ei.value.status == 3
+    g.close()
+
+
+def test_graph_replay_and_stream():
+    beg, col, g = graph("rmat13")
+    src = ib.sample_sources(beg, col, 256, seed=12)
+    ref, _ = oracle.bfs(beg, col, src)
+    import torch
+
+    out = torch.empty((len(src), len(beg) - 1), dtype=torch.uint8, device="cuda")
+    s = torch.cuda.Stream()
+    g.set_stream(s.cuda_stream)
+    try:
+        for it in range(3):
+            out.fill_(7)
+            res = g.run(src, width=128, use_graph=1, on_device=True, out_ptr=out.data_ptr())
+            s.synchronize()
+            assert np.array_equal(out.cpu().numpy(), ref)
+            if it > 0:
+                assert res.stats["gpu_launches"] == 1
+    finally:
+        g.set_stream(None)
+
+
+def test_device_output_vertex_major():
+    import torch
+
+    beg, col, g = graph("rmat10")
+    src = ib.sample_sources(beg, col, 100, seed=13)
+    V = len(beg) - 1
+    out = torch.empty(len(src) * V, dtype=torch.uint8, device="cuda")
+    g.run(src, width=128, layout=ib.LAYOUT_VERTEX_MAJOR, on_device=True, out_ptr=out.data_ptr())
+    got = out.cpu().numpy().reshape(V, len(src)).T
+    ref, _ = oracle.bfs(beg, col, src)
+    assert np.array_equal(got, ref)
+
+
+def test_barrier_timeout_is_reported():
+    """A withheld grid-barrier arrival makes every bounded wait run out; the
+    run returns IBFS_ERR_TIMEOUT and the context stays usable."""
+    beg, col, g = graph("rmat10")
+    src = ib.sample_sources(beg, col, 64, seed=1)
+    with pytest.raises(ib.IbfsError) as ei:
+        g.run(src, width=64, mode=ib.MODE_PERSISTENT, debug_withhold=1, timeout_ms=200)
+    assert ei.value.status == 6
+    run_and_check(beg, col, g, src, width=64, mode=ib.MODE_PERSISTENT)
+
+
+def test_bytes_alg_matches_oracle():
+    import torch
+
+    beg, col, g = graph("rmat10")
+    src = ib.sample_sources(beg, col, 64, seed=21)
+    ref, _ = oracle.bfs(beg, col, src)
+    dev = torch.from_numpy(ref).cuda()
+    for w in (64, 128):
+        assert g.bytes_alg(dev.data_ptr(), len(src), 1, w) == oracle.bytes_alg(beg, col, ref, w)
