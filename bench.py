@@ -1,0 +1,418 @@
+"""Benchmark of the concurrent multi-source BFS (one JSON line on rank 0).
+
+Default workload: R-MAT scale 24 (16.8M vertices, edge factor 16, a/b/c/d =
+.57/.19/.19/.05, ~537M directed CSR entries), 1024 sources from the giant
+component, GroupBy into 8 batches of 128 sources with 128-bit status words,
+one persistent launch per run replayed from a CUDA graph.  A step is one
+whole run over all 1024 sources.
+
+  value   aggregate GTEPS (sum over sources of the edges of the vertices each
+          source reached, validate.h:59-76, / device time) with the CSR and the
+          sources resident and the depths left in HBM;
+  e2e     the same metric through the C ABI with HOST buffers: source ids
+          uploaded from pinned memory and every depth byte copied back to
+          pinned host memory inside the timed region;
+  roofline: algorithmic bytes of the run (the implementation-independent byte
+          model, computed on the GPU from the depths) / the persistent kernel's
+          average event-timed duration, against MEASURED_PEAKS.json hbm_gbs.
+
+``--impl reference`` times the CPU oracle (the project's restatement of the
+reference's sequential BFS; the reference has no runnable CPU BFS of its own)
+on all host cores over a bounded sample of the same workload.
+
+Multi-GPU (torchrun): sources shard across ranks -- every rank runs its own
+1024 sources on a full replica of the graph, no collective on the data path
+(weak scaling); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "c1": dict(kind="rmat", scale=16, ef=16, seed=1, nsrc=128, src_seed=1, giant=False,
+               workload="rmat-s16-ef16-128src"),
+    "c2": dict(kind="rmat", scale=22, ef=16, seed=2, nsrc=512, src_seed=2, giant=True,
+               workload="rmat-s22-ef16-512src"),
+    "c3": dict(kind="rmat", scale=24, ef=16, seed=3, nsrc=1024, src_seed=3, giant=True,
+               workload="rmat-s24-ef16-1024src-groupby"),
+    "c4": dict(kind="grid", rows=4096, cols=4096, seed=4, nsrc=256, src_seed=4, giant=False,
+               workload="grid-4096x4096-del5pct-sc0.1pct-256src"),
+    "c5": dict(kind="chunglu", n=3_070_000, m=117_000_000, seed=5, nsrc=256, src_seed=5,
+               giant=False, workload="chunglu-3.07M-117M-g2.1-256src"),
+}
+
+SMI_FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def make_graph(cfg):
+    import ibfs_b200 as ib
+
+    if cfg["kind"] == "rmat":
+        return ib.gen_rmat(cfg["scale"], cfg["ef"], 0.57, 0.19, 0.19, seed=cfg["seed"])
+    if cfg["kind"] == "grid":
+        return ib.gen_grid(cfg["rows"], cfg["cols"], 0.05, 0.001, seed=cfg["seed"])
+    return ib.gen_chung_lu(cfg["n"], cfg["m"], 2.1, 33000.0, seed=cfg["seed"])
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        try:
+            d = json.load(open(p))
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={SMI_FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = max(mx, float(r[1]))
+            except (ValueError, IndexError):
+                continue
+            for i, nm in enumerate(names):
+                if len(r) > 4 + i and r[4 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def cpu_sample(beg, col, src, budget_s: float = 20.0):
+    """Time the oracle on all host cores over a bounded sample of sources."""
+    import oracle
+
+    threads = oracle.max_threads()
+    k = max(threads, 8)
+    k = min(k, len(src))
+    # calibrate on one wave so that the sample ends near budget_s
+    t0 = time.perf_counter()
+    d, _ = oracle.bfs(beg, col, src[:k], 1, threads)
+    dt = time.perf_counter() - t0
+    edges = oracle.teps(beg, d)
+    waves = max(1, min(int(budget_s / max(dt, 1e-3)), len(src) // k))
+    if waves > 1:
+        sub = src[:k * waves]
+        t0 = time.perf_counter()
+        d, _ = oracle.bfs(beg, col, sub, 1, threads)
+        dt = time.perf_counter() - t0
+        edges = oracle.teps(beg, d)
+        k = len(sub)
+    return edges / dt / 1e9, threads, k, dt
+
+
+def run_reference(args, cfg):
+    world, rank, local = dist_setup(args)
+    if rank != 0:
+        return
+    import ibfs_b200 as ib
+
+    beg, col = make_graph(cfg)
+    src = ib.sample_sources(beg, col, cfg["nsrc"], cfg["src_seed"], giant_component=cfg["giant"])
+    vals = []
+    for i in range(args.warmup + args.steps):
+        g, thr, k, dt = cpu_sample(beg, col, src, budget_s=args.ref_budget)
+        if i >= args.warmup:
+            vals.append(g)
+    v = statistics.median(vals)
+    line = {
+        "metric": "aggregate GTEPS", "value": round(v, 4), "unit": "GTEPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
+        "impl": "reference",
+        "config": {"workload": cfg["workload"], "sources": cfg["nsrc"], "parallelism": "cpu-openmp"},
+        "cpu_baseline": {"value": round(v, 4), "unit": "GTEPS", "cores": thr, "kind": "port",
+                         "sample": f"{k} of {cfg['nsrc']} sources per step, oracle BFS on {thr} "
+                                   f"threads"},
+        "e2e": {"value": round(v, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, cfg):
+    world, rank, local = dist_setup(args)
+    import torch
+
+    import ibfs_b200 as ib
+
+    torch.cuda.set_device(local)
+    torch.cuda.init()
+    t_gen = time.perf_counter()
+    beg, col = make_graph(cfg)
+    src = ib.sample_sources(beg, col, cfg["nsrc"], cfg["src_seed"] + 1000 * rank,
+                            giant_component=cfg["giant"])
+    t_gen = time.perf_counter() - t_gen
+    V = len(beg) - 1
+    g = ib.Graph.from_csr(beg, col, device=local)
+    stream = torch.cuda.Stream(device=local)
+    g.set_stream(stream.cuda_stream)
+    opts = ib.default_opts(width=args.width, concurrent=args.concurrent,
+                           mode=ib.MODE_PERSISTENT if args.mode == "persistent" else ib.MODE_PLAIN,
+                           groupby=0 if args.no_groupby else 1, use_graph=0 if args.no_graph else 1,
+                           depth_bytes=1, groups=args.groups)
+    n = len(src)
+    out = torch.empty((n, V), dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step():
+        return g.run(src, opts, on_device=True, out_ptr=out.data_ptr())
+
+    for _ in range(max(args.warmup, 3)):
+        res = step()
+    stream.synchronize()
+    barrier(world)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kern_ms, launches, edges = [], 0, 0
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier(world)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            res = step()
+            kern_ms.append(res.stats["device_ms"])
+            launches += res.stats["gpu_launches"]
+            edges += res.stats["traversed_edges"]
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+    t_ms = ev0.elapsed_time(ev1)
+    t_ms_max = max_over_ranks(t_ms, world)
+    edges_all = sum_over_ranks(float(edges), world)
+    value = edges_all / (t_ms_max / 1e3) / 1e9
+    kernel_ms = statistics.mean(kern_ms)
+
+    # ---- roofline: algorithmic bytes of one run (outside the timed region)
+    bytes_alg = None
+    if not args.no_roofline:
+        order = g.groupby(src) if not args.no_groupby else src
+        pos = {}
+        rows = []
+        idx_of = {}
+        for i, s in enumerate(src.tolist()):
+            idx_of.setdefault(s, []).append(i)
+        for s in order.tolist():
+            rows.append(idx_of[s].pop(0))
+        C = args.concurrent or args.width
+        total = 0
+        for b0 in range(0, n, C):
+            sel = torch.tensor(rows[b0:b0 + C], device=out.device)
+            blk = out.index_select(0, sel).contiguous()
+            total += g.bytes_alg(blk.data_ptr(), blk.shape[0], 1, args.width)
+            del blk
+        bytes_alg = total
+    pk, pk_kind = peaks()
+    roof = None
+    if bytes_alg is not None:
+        ach = bytes_alg / (kernel_ms / 1e3) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tp):
+            try:
+                traffic = json.load(open(tp)).get(cfg["workload"])
+            except Exception:
+                traffic = None
+        roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": pk, "unit": "GB/s",
+                "frac": round(ach / pk, 4), "traffic": traffic,
+                "peak_source": f"{pk_kind} MEASURED_PEAKS.json hbm_gbs" if pk_kind == "measured"
+                else "fallback 6650 GB/s",
+                "bytes_alg_per_launch": bytes_alg, "kernel_ms": round(kernel_ms, 4),
+                "kernel": "persistent_kernel<4>" if args.width == 128 else f"persistent_kernel(W={args.width})"}
+
+    # ---- e2e: host buffers through the C ABI
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty((n, V), dtype=torch.uint8, pin_memory=True)
+        hptr = host.data_ptr()
+        import ctypes
+
+        opts_h = ib.Opts.from_buffer_copy(opts)
+        st = ib.Stats()
+        src_pinned = torch.from_numpy(np.ascontiguousarray(src)).pin_memory()
+        lib = ib.api._lib()
+
+        def hstep():
+            rc = lib.ibfs_run(g.handle, ctypes.c_void_p(src_pinned.data_ptr()), n,
+                              ctypes.byref(opts_h), ctypes.c_void_p(hptr), 0, 0, ctypes.byref(st))
+            if rc != 0:
+                raise ib.IbfsError(rc, "ibfs_run (e2e)")
+            return st.traversed_edges
+
+        for _ in range(max(1, min(args.warmup, 2))):
+            hstep()
+        barrier(world)
+        e_steps = max(1, min(args.steps, args.e2e_steps))
+        t0 = time.perf_counter()
+        ee = 0
+        for _ in range(e_steps):
+            ee += hstep()
+        t_e = time.perf_counter() - t0
+        t_e = max_over_ranks(t_e, world)
+        ee_all = sum_over_ranks(float(ee), world)
+        e2e = {"value": round(ee_all / t_e / 1e9, 4), "unit": "GTEPS",
+               "h2d_bytes_per_step": int(n * 4), "d2h_bytes_per_step": int(n * V),
+               "steps": e_steps}
+        ok = np.array_equal(host.numpy()[0], out[0].cpu().numpy())
+        e2e["matches_device_run"] = bool(ok)
+        del host
+
+    # ---- CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        gcpu, thr, k, dt = cpu_sample(beg, col, src, budget_s=args.cpu_budget)
+        cpu = {"value": round(gcpu, 4), "unit": "GTEPS", "cores": thr, "kind": "port",
+               "sample": f"{k} of {n} sources, oracle BFS (restated sequential queue BFS, "
+                         f"OpenMP over sources), {dt:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": "aggregate GTEPS", "value": round(value, 3), "unit": "GTEPS",
+            "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": round(t_ms_max / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generators, no dataset)",
+            "config": {"workload": cfg["workload"], "V": V, "E": int(len(col)), "sources": n,
+                       "width": args.width, "concurrent": args.concurrent or args.width,
+                       "schedule": args.mode + ("+cuda-graph" if not args.no_graph else ""),
+                       "groupby": not args.no_groupby, "parallelism": f"source-shard x{world}",
+                       "l2": "inputs larger than L2 (CSR 2.1 GB, status 268 MB/batch)",
+                       "gen_s": round(t_gen, 1), "max_level": res.stats["max_level"],
+                       "groups": res.stats["groups"], "td_levels": res.stats["td_levels"],
+                       "bu_levels": res.stats["bu_levels"]},
+            "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    g.set_stream(None)
+    g.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        barrier(world)
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
+    ap.add_argument("--width", type=int, default=128)
+    ap.add_argument("--concurrent", type=int, default=128)
+    ap.add_argument("--groups", type=int, default=0)
+    ap.add_argument("--mode", default="persistent", choices=["persistent", "plain"])
+    ap.add_argument("--no-groupby", action="store_true")
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-roofline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-budget", type=float, default=10.0)
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, cfg)
+    else:
+        run_ours(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

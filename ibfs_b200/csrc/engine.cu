@@ -223,6 +223,7 @@ __global__ void __launch_bounds__(512) k_finish(Params p, GroupBufs gb, int b) {
     cudaError_t e_ = (call);                           \
     if (e_ != cudaSuccess) {                           \
       last_cuda_error() = e_;                          \
+      (void)cudaGetLastError();                        \
       return e_ == cudaErrorMemoryAllocation ? IBFS_ERR_OOM : IBFS_ERR_CUDA; \
     }                                                  \
   } while (0)
@@ -860,7 +861,10 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     CU(cudaMemcpyAsync(g->d_groups.p, hgb, sizeof(GroupBufs) * rp.G, cudaMemcpyHostToDevice, cs));
     for (int i = 0; i < rp.G; i++) CU(cudaMemsetAsync(hgb[i].ctl, 0, sizeof(Ctl), cs));
     CU(cudaMemsetAsync(g->d_brec.p, 0, sizeof(BatchRec) * rp.nbatches, cs));
-    CU(cudaEventRecord(g->ev0, cs));
+    // inside a capture a plain cudaEventRecord only orders work; an external
+    // record becomes a real event-record node that replays time
+    if (capturing) CU(cudaEventRecordWithFlags(g->ev0, cs, cudaEventRecordExternal));
+    else CU(cudaEventRecord(g->ev0, cs));
     if (persistent) {
       cudaLaunchConfig_t cfg;
       std::memset(&cfg, 0, sizeof(cfg));
@@ -877,13 +881,9 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
       CU(cudaLaunchKernelExC(&cfg, persistent_for(rp.words), args));
       launches += 1;
     }
-    CU(cudaEventRecord(g->ev1, cs));
-    if (rp.host_out) {
-      if (layout == IBFS_LAYOUT_SOURCE_MAJOR || true) {
-        CU(cudaMemcpyAsync(depth_out, dout, out_bytes, cudaMemcpyDeviceToHost, cs));
-      }
-    }
-    (void)capturing;
+    if (capturing) CU(cudaEventRecordWithFlags(g->ev1, cs, cudaEventRecordExternal));
+    else CU(cudaEventRecord(g->ev1, cs));
+    if (rp.host_out) CU(cudaMemcpyAsync(depth_out, dout, out_bytes, cudaMemcpyDeviceToHost, cs));
     return IBFS_OK;
   };
 
@@ -1007,8 +1007,11 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   }
   const BatchRec* br = g->h_brec.as<BatchRec>();
   if (st) {
-    float ms = 0;
-    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    float ms = -1.0f;
+    if (cudaEventElapsedTime(&ms, g->ev0, g->ev1) != cudaSuccess) {
+      (void)cudaGetLastError();  // leave no stale error in the shared runtime
+      ms = -1.0f;
+    }
     st->n_sources = n;
     st->n_batches = rp.nbatches;
     st->depth_bytes = db;
