@@ -85,6 +85,8 @@ _SIGS = [
     ("ibfs_set_stream", C.c_int, [_P, _P]),
     ("ibfs_teps", C.c_int, [_P, _P, C.c_int64, C.c_int32, _I64P]),
     ("ibfs_bytes_alg", C.c_int, [_P, _P, C.c_int64, C.c_int32, C.c_int32, _I64P]),
+    ("ibfs_run_static_scratch", C.c_int, [_P, _P, C.c_int64, C.c_int64, _P, C.c_int64, C.c_int32,
+                                          _P, _P, _I64P]),
     ("ibfs_gen_rmat", C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                 C.c_uint64, C.POINTER(_P), C.POINTER(_P), _I64P, _I64P]),
     ("ibfs_gen_grid", C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_uint64,

@@ -1045,3 +1045,30 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   }
   return IBFS_OK;
 }
+
+namespace ibfs {
+// Launch the persistent kernel for an already filled Params (used by the
+// static-scratch entry point in noalloc.cu; allocates nothing).
+cudaError_t launch_persistent_params(const Params& p, int words, int grid, int threads,
+                                     size_t smem, cudaStream_t s) {
+  cudaLaunchConfig_t cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  Params q = p;
+  void* args[] = {&q};
+  return cudaLaunchKernelExC(&cfg, persistent_for(words), args);
+}
+
+cudaError_t persistent_occupancy(int words, int threads, size_t smem, int* per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, persistent_for(words), threads,
+                                                       smem);
+}
+}  // namespace ibfs

@@ -5,6 +5,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "../../include/ibfs.h"
 
 namespace ibfs {
@@ -39,4 +41,12 @@ ibfs_status validate_csr(const int64_t* beg, const int32_t* col, int64_t V,
 void groupby_host(const int64_t* beg, const int32_t* col, int64_t V,
                   const int32_t* src, int64_t n, int32_t* out);
 
+}  // namespace ibfs
+
+namespace ibfs {
+struct Params;
+// engine.cu: launch helpers shared with the static-scratch entry point.
+cudaError_t launch_persistent_params(const Params& p, int words, int grid, int threads,
+                                     size_t smem, cudaStream_t s);
+cudaError_t persistent_occupancy(int words, int threads, size_t smem, int* per_sm);
 }  // namespace ibfs

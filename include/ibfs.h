@@ -175,6 +175,28 @@ ibfs_status ibfs_teps(const ibfs_graph *g, const void *depth_host, int64_t n,
 ibfs_status ibfs_bytes_alg(ibfs_graph *g, const void *depth_dev, int64_t n,
                            int32_t depth_bytes, int32_t width, int64_t *bytes);
 
+/* No counterpart in the reference.  Concurrent BFS that allocates nothing,
+   for callers that cannot call cudaMalloc (a plug-in inside a process whose
+   allocator owns all device memory, a latency-critical path that may not
+   stall in cudaMalloc, a deployment that forbids allocation after start-up).
+   All inputs and the output are the caller's device memory: the CSR
+   (beg_dev int64[V+1], col_dev int32[E]), the source ids src_dev int32[n]
+   and depth_dev, which receives uint8 depths (INFTY 255) in the vertex-major
+   layout with batches of `width` sources: batch b at b*V*width, rows of
+   min(width, n - b*width) bytes.  Scratch comes from one fixed 64 MiB device
+   array inside the library (held by every GPU that loads it, until exit);
+   graphs whose scratch does not fit, more than 16 batches, or a level past
+   254 return IBFS_ERR_RANGE.  Runs on the calling thread's current device;
+   the first call on a device looks up the array's address, so make that
+   first call before any stream capture.  Calls share the array: calls whose
+   work overlaps on one GPU race and must be serialised by the caller.
+   Synchronises `cuda_stream` (a cudaStream_t, NULL = legacy stream) before
+   returning; traversed_edges (may be NULL) receives the TEPS numerator. */
+ibfs_status ibfs_run_static_scratch(const int64_t *beg_dev, const int32_t *col_dev,
+                                    int64_t V, int64_t E, const int32_t *src_dev,
+                                    int64_t n, int32_t width, void *depth_dev,
+                                    void *cuda_stream, int64_t *traversed_edges);
+
 /* ---- synthetic inputs (seeded, deterministic, host) -------------------- */
 /* Each generator symmetrises, drops self-loops, dedupes and sorts every
    adjacency list.  Arrays are malloc'ed by the library; free with ibfs_free. */
