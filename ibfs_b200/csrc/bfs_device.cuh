@@ -13,14 +13,20 @@
 //   expand   top-down push over the joint frontier queues (expander.cuh:
 //            140-331) or bottom-up pull over all vertices (expander.cuh:
 //            341-489); both mark changed vertices in a 1-bit-per-vertex
-//            bitmap `chg` (V/8 bytes, L2 resident);
-//   inspect  walks the bitmap only: new bits = curr & ~last, writes the
-//            depth bytes of the new bits, last = curr, and accumulates the
-//            direction-switch counters.  Replaces the O(V) count/scan/gather
-//            passes of inspector.cuh:63-525 and scan.cuh:455-655;
+//            bitmap (V/8 bytes, L2 resident), double-buffered by level parity
+//            so that the bottom-up pull can skip neighbours outside the
+//            previous frontier;
+//   inspect  walks the bitmap only: new bits = curr & ~last, last = curr,
+//            ORs the new bits into the depth bit-planes of the level number,
+//            and accumulates the direction-switch counters.  Replaces the
+//            O(V) count/scan/gather passes of inspector.cuh:63-525,
+//            scan.cuh:455-655 and the per-level depth_merge writes of
+//            inspector.cuh:8-56,113-120;
 //   qbuild   (only before a top-down level) turns the bitmap into the
 //            small/medium/large queues with warp-ballot compaction
 //            (replaces td_frontier_count/td_frontier_gather).
+// After the last level one pass turns the bit-planes into the depth output
+// (either layout), writing every output byte exactly once.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -29,7 +35,8 @@ namespace ibfs {
 
 constexpr int kDirTD = 0;
 constexpr int kDirBU = 1;
-constexpr int kMaxWords = 8;  // W = 256
+constexpr int kMaxWords = 8;   // W = 256
+constexpr int kMaxPlanes = 16; // two-byte depths
 
 // Per-level counters, double-buffered by level parity.
 struct Par {
@@ -68,20 +75,22 @@ struct LevelRec {
 };
 
 struct GroupBufs {
-  uint32_t* last;
-  uint32_t* curr;
-  uint32_t* chg;
+  uint32_t* last;    // [Vpad][WORDS]
+  uint32_t* curr;    // [Vpad][WORDS]
+  uint32_t* chg;     // 2 bitmaps of chg_stride words (level parity)
+  uint32_t* planes;  // depth bit-planes, plane b at b*plane_stride words
   int32_t* qs;
   int32_t* qm;
   int2* ql;
   Ctl* ctl;
-  uint8_t* stage;  // vertex-major depth staging [V][C] (db bytes each)
 };
 
 struct Params {
   const int64_t* beg;
   const int32_t* col;
   int64_t V, E, nchg;
+  long long chg_stride;    // words per bitmap (nchg rounded up to 4)
+  long long plane_stride;  // words per bit-plane (Vpad * WORDS)
   const int32_t* src;      // ordered sources [n_total]
   const int32_t* out_row;  // output row of ordered source k (source-major)
   int64_t n_total;
@@ -99,7 +108,8 @@ struct Params {
   BatchRec* brec;
   LevelRec* lrec;
   int lrec_cap;
-  int vec_out;  // output rows allow 4-vertex vector stores (V % 4 == 0, aligned base)
+  int vec_out;  // vertex-major rows allow 4-byte stores (n_b*db % 4 == 0, aligned base)
+  int vec_sm;   // source-major rows allow 4-vertex stores (V % 4 == 0, aligned base)
 };
 
 // A team is the set of threads that share one batch: the whole grid in the
@@ -110,6 +120,10 @@ struct Team {
   long long warp, nwarps;
   int lane;
 };
+
+__host__ __device__ inline uint32_t* chg_at(const GroupBufs& gb, const Params& p, int level) {
+  return gb.chg + (level & 1) * p.chg_stride;
+}
 
 // ---------------------------------------------------------------------------
 // small helpers
@@ -164,19 +178,26 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 
 // Bit mask of the sources of a batch of n inside word k.
-__device__ __forceinline__ uint32_t full_word(int n, int k) {
+__host__ __device__ __forceinline__ uint32_t full_word(int n, int k) {
   const int lo = k * 32;
   if (n >= lo + 32) return 0xFFFFFFFFu;
   if (n <= lo) return 0u;
   return (1u << (n - lo)) - 1u;
 }
 
+// Number of depth bit-planes that levels 0..max_level use.
+__host__ __device__ __forceinline__ int planes_for(int max_level) {
+  int p = 0;
+  while (p < 31 && (max_level >> p) != 0) p++;
+  return p;
+}
+
 // Bounded team barrier.  All waits end: after timeout_ns the waiting CTA
 // records IBFS_ERR_TIMEOUT (6) in ctl->err and every other CTA leaves on
 // seeing a non-zero err.  Returns false when the team must stop.
 static __device__ __noinline__ bool team_barrier(Ctl* ctl, unsigned nblocks,
-                                          unsigned long long timeout_ns,
-                                          bool withhold) {
+                                                 unsigned long long timeout_ns,
+                                                 bool withhold) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -240,9 +261,11 @@ __device__ __forceinline__ void cta_or_u32(uint32_t* dst, uint32_t x) {
   }
 }
 
-__device__ __forceinline__ void store_depth(uint8_t* row, int idx, int db, int level) {
-  if (db == 1) row[idx] = (uint8_t)level;
-  else reinterpret_cast<uint16_t*>(row)[idx] = (uint16_t)level;
+__device__ __forceinline__ void zero_words(uint32_t* p, long long nwords, const Team& t) {
+  // nwords is a multiple of 4 and p 16-byte aligned (allocation padding)
+  uint4* q = reinterpret_cast<uint4*>(p);
+  const uint4 z = make_uint4(0, 0, 0, 0);
+  for (long long i = t.tid; i < nwords / 4; i += t.nthreads) __stcg(q + i, z);
 }
 
 // ---------------------------------------------------------------------------
@@ -265,25 +288,35 @@ __host__ __device__ inline int choose_dir(int next_level, int prev_dir,
 }
 
 // ---------------------------------------------------------------------------
-// Phase: seed the sources of one batch (curr bits + changed bits).
+// Phase: seed the sources of one batch (curr bits + level-0 changed bits).
 // ---------------------------------------------------------------------------
 template <int WORDS>
 __device__ void seed_phase(const Params& p, const GroupBufs& gb,
                            const int32_t* src_b, int n_b, const Team& t) {
+  uint32_t* chg0 = chg_at(gb, p, 0);
   for (long long i = t.tid; i < n_b; i += t.nthreads) {
     const int32_t v = src_b[i];
     atomicOr(gb.curr + (size_t)v * WORDS + (i >> 5), 1u << (i & 31));
-    atomicOr(gb.chg + (v >> 5), 1u << (v & 31));
+    atomicOr(chg0 + (v >> 5), 1u << (v & 31));
+  }
+}
+
+// Zero depth bit-plane b when `level` = 2^b, the first level that uses it.
+__device__ __forceinline__ void zero_plane_if_first(const Params& p, const GroupBufs& gb,
+                                                    int level, const Team& t) {
+  if (level > 0 && (level & (level - 1)) == 0) {
+    const int b = __ffs(level) - 1;
+    zero_words(gb.planes + (size_t)b * p.plane_stride, p.plane_stride, t);
   }
 }
 
 // ---------------------------------------------------------------------------
-// Phase: inspect level L (reads chg, fixes last, writes depth, counters).
+// Phase: inspect level L (reads the level-L bitmap, fixes last, updates the
+// depth bit-planes, counters).
 // ---------------------------------------------------------------------------
 template <int WORDS>
-__device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par,
-                              uint8_t* depth, int n_b, int level, bool depth_ok,
-                              const Team& t) {
+__device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par, int n_b,
+                              int level, bool depth_ok, const Team& t) {
   uint32_t full[WORDS];
 #pragma unroll
   for (int k = 0; k < WORDS; k++) full[k] = full_word(n_b, k);
@@ -291,49 +324,42 @@ __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par,
   uint32_t fm[WORDS];
 #pragma unroll
   for (int k = 0; k < WORDS; k++) fm[k] = 0;
+  const uint32_t* chg = chg_at(gb, p, level);
   const int lane = t.lane;
-  const size_t row_bytes = (size_t)n_b * p.db;
   for (long long w = t.warp; w < p.nchg; w += t.nwarps) {
-    const uint32_t bits = __ldcg(gb.chg + w);
+    const uint32_t bits = __ldcg(chg + w);
     if (!bits) continue;
     const long long v = w * 32 + lane;
-    const bool mine = (bits >> lane) & 1u;
-    uint32_t nb[WORDS];
+    if (!((bits >> lane) & 1u)) continue;
+    uint32_t c[WORDS], l[WORDS], nb[WORDS];
+    ld_status<WORDS>(gb.curr + (size_t)v * WORDS, c);
+    ld_status<WORDS>(gb.last + (size_t)v * WORDS, l);
+    bool comp = true;
+    uint32_t pop = 0;
 #pragma unroll
-    for (int k = 0; k < WORDS; k++) nb[k] = 0;
-    if (mine) {
-      uint32_t c[WORDS], l[WORDS];
-      ld_status<WORDS>(gb.curr + (size_t)v * WORDS, c);
-      ld_status<WORDS>(gb.last + (size_t)v * WORDS, l);
-      bool comp = true;
-      uint32_t pop = 0;
-#pragma unroll
-      for (int k = 0; k < WORDS; k++) {
-        nb[k] = c[k] & ~l[k];
-        comp = comp && (c[k] == full[k]);
-        pop += __popc(nb[k]);
-        fm[k] |= nb[k];
-      }
-      st_status<WORDS>(gb.last + (size_t)v * WORDS, c);
-      const long long deg = p.beg[v + 1] - p.beg[v];
-      mf += deg;
-      cnt += 1;
-      teps += (unsigned long long)deg * pop;
-      if (comp) cdeg += deg;
+    for (int k = 0; k < WORDS; k++) {
+      nb[k] = c[k] & ~l[k];
+      comp = comp && (c[k] == full[k]);
+      pop += __popc(nb[k]);
+      fm[k] |= nb[k];
     }
-    if (!depth_ok) continue;
-    // Depth bytes: the warp writes one changed vertex's row at a time; lane
-    // l owns sources l, l+32, ... so every store instruction is one
-    // coalesced (byte-masked) 32-source segment of the row.
-    uint32_t rem = bits;
-    while (rem) {
-      const int j = __ffs(rem) - 1;
-      rem &= rem - 1;
-      uint8_t* row = depth + (size_t)(w * 32 + j) * row_bytes;
+    st_status<WORDS>(gb.last + (size_t)v * WORDS, c);
+    const long long deg = p.beg[v + 1] - p.beg[v];
+    mf += deg;
+    cnt += 1;
+    teps += (unsigned long long)deg * pop;
+    if (comp) cdeg += deg;
+    if (depth_ok) {
+      // depth(v, s) = level for the new bits: OR them into the planes of
+      // the level's set bits (one coalesced read-modify-write per plane).
+      for (int b = 0; (level >> b) != 0; b++) {
+        if (!((level >> b) & 1)) continue;
+        uint32_t* q = gb.planes + (size_t)b * p.plane_stride + (size_t)v * WORDS;
+        uint32_t x[WORDS];
+        ld_status<WORDS>(q, x);
 #pragma unroll
-      for (int k = 0; k < WORDS; k++) {
-        const uint32_t x = __shfl_sync(0xFFFFFFFFu, nb[k], j);
-        if ((x >> lane) & 1u) store_depth(row, k * 32 + lane, p.db, level);
+        for (int k = 0; k < WORDS; k++) x[k] |= nb[k];
+        st_status<WORDS>(q, x);
       }
     }
   }
@@ -347,18 +373,21 @@ __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par,
 }
 
 // ---------------------------------------------------------------------------
-// Phase: build the joint frontier queues for a top-down level from chg
-// (warp-ballot compaction, degree classes as td_inspect, inspector.cuh:
-// 534-626: deg < sml -> small, deg > lrg -> large, else medium, deg 0
-// dropped).  Large vertices are cut into chunks of p.chunk edges.  Clears
-// the bitmap words it reads.
+// Phase: build the joint frontier queues for top-down level L from the
+// level-(L-1) bitmap (warp-ballot compaction, degree classes as td_inspect,
+// inspector.cuh:534-626: deg < sml -> small, deg > lrg -> large, else
+// medium, deg 0 dropped).  Large vertices are cut into chunks of p.chunk
+// edges.  Clears the level-L bitmap that the top-down pass will fill.
 // ---------------------------------------------------------------------------
-__device__ inline void qbuild_phase(const Params& p, const GroupBufs& gb,
+__device__ inline void qbuild_phase(const Params& p, const GroupBufs& gb, int level,
                                     int32_t* qc, const Team& t) {
   const int lane = t.lane;
   const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t* prev = chg_at(gb, p, level - 1);
+  uint32_t* next = chg_at(gb, p, level);
   for (long long w = t.warp; w < p.nchg; w += t.nwarps) {
-    const uint32_t bits = __ldcg(gb.chg + w);
+    const uint32_t bits = __ldcg(prev + w);
+    if (lane == 0) __stcg(next + w, 0u);
     if (!bits) continue;
     const long long v = w * 32 + lane;
     const bool mine = (bits >> lane) & 1u;
@@ -396,7 +425,6 @@ __device__ inline void qbuild_phase(const Params& p, const GroupBufs& gb,
       const int first = base + incl - nch;
       for (int c = 0; c < nch; c++) gb.ql[first + c] = make_int2((int)v, c);
     }
-    if (lane == 0) __stcg(gb.chg + w, 0u);
   }
 }
 
@@ -404,7 +432,7 @@ __device__ inline void qbuild_phase(const Params& p, const GroupBufs& gb,
 // The status read goes to L2 (ld.cg): it only filters atomics, a stale
 // value has fewer bits and just costs one more atomic.
 template <int WORDS>
-__device__ __forceinline__ void td_push(const GroupBufs& gb, int32_t u,
+__device__ __forceinline__ void td_push(const GroupBufs& gb, uint32_t* chg, int32_t u,
                                         const uint32_t (&P)[WORDS]) {
   uint32_t s[WORDS];
   ld_status<WORDS>(gb.curr + (size_t)u * WORDS, s);
@@ -429,7 +457,7 @@ __device__ __forceinline__ void td_push(const GroupBufs& gb, int32_t u,
     }
   }
   if (changed) {
-    uint32_t* cw = gb.chg + (u >> 5);
+    uint32_t* cw = chg + (u >> 5);
     const uint32_t bit = 1u << (u & 31);
     if (!(__ldcg(cw) & bit)) atomicOr(cw, bit);
   }
@@ -442,8 +470,9 @@ __device__ __forceinline__ void td_push(const GroupBufs& gb, int32_t u,
 // small vertex (td_expand_thd, expander.cuh:140-199).
 // ---------------------------------------------------------------------------
 template <int WORDS>
-__device__ void td_phase(const Params& p, const GroupBufs& gb, const int32_t* qc,
+__device__ void td_phase(const Params& p, const GroupBufs& gb, int level, const int32_t* qc,
                          const Team& t) {
+  uint32_t* chg = chg_at(gb, p, level);
   const int nS = __ldcg(qc + 0), nM = __ldcg(qc + 1), nL = __ldcg(qc + 2);
   for (int c = t.block; c < nL; c += t.nblocks) {
     const int2 d = gb.ql[c];
@@ -453,39 +482,45 @@ __device__ void td_phase(const Params& p, const GroupBufs& gb, const int32_t* qc
     const long long b1 = min(e_end, b0 + (long long)p.chunk);
     uint32_t P[WORDS];
     ld_status<WORDS>(gb.last + (size_t)v * WORDS, P);
-    for (long long e = b0 + threadIdx.x; e < b1; e += blockDim.x) td_push<WORDS>(gb, p.col[e], P);
+    for (long long e = b0 + threadIdx.x; e < b1; e += blockDim.x)
+      td_push<WORDS>(gb, chg, p.col[e], P);
   }
   for (long long i = t.warp; i < nM; i += t.nwarps) {
     const int32_t v = gb.qm[i];
     uint32_t P[WORDS];
     ld_status<WORDS>(gb.last + (size_t)v * WORDS, P);
     const long long b1 = p.beg[v + 1];
-    for (long long e = p.beg[v] + t.lane; e < b1; e += 32) td_push<WORDS>(gb, p.col[e], P);
+    for (long long e = p.beg[v] + t.lane; e < b1; e += 32) td_push<WORDS>(gb, chg, p.col[e], P);
   }
   for (long long i = t.tid; i < nS; i += t.nthreads) {
     const int32_t v = gb.qs[i];
     uint32_t P[WORDS];
     ld_status<WORDS>(gb.last + (size_t)v * WORDS, P);
     const long long b1 = p.beg[v + 1];
-    for (long long e = p.beg[v]; e < b1; e++) td_push<WORDS>(gb, p.col[e], P);
+    for (long long e = p.beg[v]; e < b1; e++) td_push<WORDS>(gb, chg, p.col[e], P);
   }
 }
 
 // ---------------------------------------------------------------------------
 // Phase: bottom-up level L.  Every vertex that still lacks a bit of the
-// previous level's frontier mask ORs the `last` words of its neighbours and
-// stops as soon as no frontier bit is missing (the early exit of
-// expander.cu:298,348, generalised from "all bits" to "all bits any frontier
-// vertex carries").  Low-degree vertices scan with one thread
-// (sw_expand_thd, expander.cuh:431-489), the rest with the whole warp and a
-// warp OR-reduction (sw_expand_warp, expander.cuh:341-422).
+// previous level's frontier mask ORs the `last` words of those neighbours
+// that were in the previous frontier (a bit can only come from a vertex
+// that gained it at level L-1; the level-(L-1) bitmap, L2 resident, filters
+// the others before their status word is read) and stops as soon as no
+// frontier bit is missing -- the early exit of expander.cu:298,348,
+// generalised from "all bits" to "all bits any frontier vertex carries".
+// Low-degree vertices scan with one thread (sw_expand_thd, expander.cuh:
+// 431-489), the rest with the whole warp and a warp OR-reduction
+// (sw_expand_warp, expander.cuh:341-422).
 // ---------------------------------------------------------------------------
 template <int WORDS>
-__device__ void bu_phase(const Params& p, const GroupBufs& gb,
+__device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
                          const uint32_t* fmask_g, const Team& t) {
   uint32_t fm[WORDS];
 #pragma unroll
   for (int k = 0; k < WORDS; k++) fm[k] = __ldcg(fmask_g + k);
+  const uint32_t* front = chg_at(gb, p, level - 1);
+  uint32_t* out = chg_at(gb, p, level);
   const int lane = t.lane;
   for (long long base = t.warp * 32; base < p.V; base += t.nwarps * 32) {
     const long long v = base + lane;
@@ -509,13 +544,29 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb,
     need = need && valid && (b1 > b0);
     const bool small = need && (b1 - b0) <= p.but;
     if (small) {
-      for (long long e = b0; e < b1; e++) {
-        uint32_t x[WORDS];
-        ld_status<WORDS>(gb.last + (size_t)p.col[e] * WORDS, x);
+      // four neighbours in flight per step: the scan is latency bound
+      for (long long e = b0; e < b1; e += 4) {
+        int32_t u[4];
+        bool f[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) u[i] = (e + i < b1) ? p.col[e + i] : -1;
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+          f[i] = u[i] >= 0 && ((__ldcg(front + (u[i] >> 5)) >> (u[i] & 31)) & 1u);
+        uint32_t x[4][WORDS];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          if (f[i]) {
+            ld_status<WORDS>(gb.last + (size_t)u[i] * WORDS, x[i]);
+          } else {
+#pragma unroll
+            for (int k = 0; k < WORDS; k++) x[i][k] = 0;
+          }
+        }
         bool miss = false;
 #pragma unroll
         for (int k = 0; k < WORDS; k++) {
-          acc[k] |= x[k];
+          acc[k] |= x[0][k] | x[1][k] | x[2][k] | x[3][k];
           miss |= (fm[k] & ~acc[k]) != 0u;
         }
         if (!miss) break;
@@ -532,11 +583,12 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb,
       for (int k = 0; k < WORDS; k++) a[k] = __shfl_sync(0xFFFFFFFFu, acc[k], j);
       for (long long e = e0; e < e1; e += 32) {
         uint32_t x[WORDS];
-        if (e + lane < e1) {
-          ld_status<WORDS>(gb.last + (size_t)p.col[e + lane] * WORDS, x);
-        } else {
 #pragma unroll
-          for (int k = 0; k < WORDS; k++) x[k] = 0;
+        for (int k = 0; k < WORDS; k++) x[k] = 0;
+        if (e + lane < e1) {
+          const int32_t u = p.col[e + lane];
+          if ((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u)
+            ld_status<WORDS>(gb.last + (size_t)u * WORDS, x);
         }
         bool miss = false;
 #pragma unroll
@@ -557,123 +609,166 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb,
     ch = ch && need;
     if (ch) st_status<WORDS>(gb.curr + (size_t)v * WORDS, acc);
     const uint32_t bal = __ballot_sync(0xFFFFFFFFu, ch);
-    if (lane == 0) __stcg(gb.chg + (base >> 5), bal);
+    if (lane == 0) __stcg(out + (base >> 5), bal);
   }
 }
 
 // ---------------------------------------------------------------------------
-// Phase: finish one batch's depth output.  Depth bytes of (v, s) were
-// written only at the level s reached v; unreached pairs are filled with
-// INFTY here (255 / 65535, comm.h:120) from the final status bits, so no
-// byte is written twice and there is no up-front fill pass.
-//   vertex-major: in place in `stage` ([V][n_b]);
-//   source-major: transpose `stage` into out rows out_row[k0 + j] through a
-//   shared-memory tile of 128 vertices.
+// Phase: write one batch's depths from the bit-planes.  Depth of (v, s) =
+// the number whose bit b is bit s of plane b, INFTY (255 / 65535,
+// comm.h:120) when bit s of the final status is clear.  Every output byte is
+// written once, in whole sectors.
+//   source-major: rows out_row[...] of V depths;
+//   vertex-major: the batch block [V][n_b] (depth_merge, inspector.cuh:48).
 // ---------------------------------------------------------------------------
-template <int WORDS>
-__device__ void finish_vertex_major(const Params& p, const GroupBufs& gb,
-                                    uint8_t* depth, int n_b, const Team& t) {
+
+// 4 bits -> the low bit of 4 bytes (bit i -> bit 8i).
+__device__ __forceinline__ uint32_t nib_to_bytes(uint32_t nib) {
+  return (nib * 0x00204081u) & 0x01010101u;
+}
+// 8 bits -> every 4th bit of a word (bit r -> bit 4r).
+__device__ __forceinline__ uint32_t spread8(uint32_t b8) {
+  uint32_t x = b8 & 0xFFu;
+  x = (x | (x << 12)) & 0x000F000Fu;
+  x = (x | (x << 6)) & 0x03030303u;
+  x = (x | (x << 3)) & 0x11111111u;
+  return x;
+}
+// Interleave the words of 4 vertices: bit 4r+i of y[q] = bit 8q+r of x[i],
+// so nibble r of y[q] holds source 8q+r for the 4 vertices.
+__device__ __forceinline__ void interleave4(const uint32_t (&x)[4], uint32_t (&y)[4]) {
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+    y[q] = spread8(x[0] >> (8 * q)) | (spread8(x[1] >> (8 * q)) << 1) |
+           (spread8(x[2] >> (8 * q)) << 2) | (spread8(x[3] >> (8 * q)) << 3);
+}
+
+// Source-major, one-byte depths, NP planes known at compile time: lane =
+// 4 consecutive vertices, one 4-byte store per source.
+template <int WORDS, int NP>
+__device__ void output_sm_u8(const Params& p, const GroupBufs& gb, const int32_t* rows, int n_b,
+                             const Team& t) {
   const int lane = t.lane;
-  const size_t row_bytes = (size_t)n_b * p.db;
-  const uint16_t inf = p.db == 1 ? 0xFFu : 0xFFFFu;
-  for (long long base = t.warp * 32; base < p.V; base += t.nwarps * 32) {
-    const long long v = base + lane;
-    uint32_t l[WORDS];
-    bool incomplete = false;
-    if (v < p.V) {
-      ld_status<WORDS>(gb.last + (size_t)v * WORDS, l);
+  for (long long base = t.warp * 128; base < p.V; base += t.nwarps * 128) {
+    const long long v0 = base + 4 * lane;
+    const bool full4 = p.vec_sm && v0 + 3 < p.V;
+#pragma unroll 1
+    for (int k = 0; k < WORDS && k * 32 < n_b; k++) {
+      uint32_t x[4], ys[4], yp[NP > 0 ? NP : 1][4];
 #pragma unroll
-      for (int k = 0; k < WORDS; k++) incomplete |= (full_word(n_b, k) & ~l[k]) != 0u;
-    }
-    uint32_t todo = __ballot_sync(0xFFFFFFFFu, incomplete);
-    while (todo) {
-      const int j = __ffs(todo) - 1;
-      todo &= todo - 1;
-      uint8_t* row = depth + (size_t)(base + j) * row_bytes;
+      for (int i = 0; i < 4; i++) x[i] = v0 + i < p.V ? gb.last[(size_t)(v0 + i) * WORDS + k] : 0u;
+      interleave4(x, ys);
 #pragma unroll
-      for (int k = 0; k < WORDS; k++) {
-        const uint32_t x = __shfl_sync(0xFFFFFFFFu, l[k], j);
-        const int s = k * 32 + lane;
-        if (s < n_b && !((x >> lane) & 1u)) store_depth(row, s, p.db, inf);
+      for (int b = 0; b < NP; b++) {
+        const uint32_t* pl = gb.planes + (size_t)b * p.plane_stride;
+#pragma unroll
+        for (int i = 0; i < 4; i++) x[i] = v0 + i < p.V ? pl[(size_t)(v0 + i) * WORDS + k] : 0u;
+        interleave4(x, yp[b]);
+      }
+      const int js = min(32, n_b - k * 32);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+          const int j = q * 8 + r;
+          if (j < js) {
+            uint32_t w = nib_to_bytes(~(ys[q] >> (4 * r)) & 0xFu) * 0xFFu;
+#pragma unroll
+            for (int b = 0; b < NP; b++) w |= nib_to_bytes((yp[b][q] >> (4 * r)) & 0xFu) << b;
+            uint8_t* row = p.out + (size_t)rows[k * 32 + j] * (size_t)p.V;
+            if (full4) {
+              *reinterpret_cast<uint32_t*>(row + v0) = w;
+            } else {
+              for (int i = 0; i < 4; i++)
+                if (v0 + i < p.V) row[v0 + i] = (uint8_t)(w >> (8 * i));
+            }
+          }
+        }
       }
     }
   }
 }
 
-constexpr int kTileV = 128;
+// Vertex-major, one-byte depths: lane = vertex, 4 sources per store.
+template <int WORDS, int NP>
+__device__ void output_vm_u8(const Params& p, const GroupBufs& gb, uint8_t* depth_vm, int n_b,
+                             const Team& t) {
+  const bool vec = p.vec_out && (n_b % 4 == 0);
+  for (long long v = t.tid; v < p.V; v += t.nthreads) {
+    uint8_t* row = depth_vm + (size_t)v * n_b;
+#pragma unroll 1
+    for (int k = 0; k < WORDS && k * 32 < n_b; k++) {
+      const uint32_t st = gb.last[(size_t)v * WORDS + k];
+      uint32_t pw[NP > 0 ? NP : 1];
+#pragma unroll
+      for (int b = 0; b < NP; b++) pw[b] = gb.planes[(size_t)b * p.plane_stride + (size_t)v * WORDS + k];
+      const int js = min(32, n_b - k * 32);
+#pragma unroll
+      for (int j4 = 0; j4 < 8; j4++) {
+        if (j4 * 4 < js) {
+          uint32_t w = nib_to_bytes(~(st >> (4 * j4)) & 0xFu) * 0xFFu;
+#pragma unroll
+          for (int b = 0; b < NP; b++) w |= nib_to_bytes((pw[b] >> (4 * j4)) & 0xFu) << b;
+          if (vec && j4 * 4 + 4 <= js) {
+            *reinterpret_cast<uint32_t*>(row + k * 32 + j4 * 4) = w;
+          } else {
+            for (int i = 0; i < 4 && j4 * 4 + i < js; i++) row[k * 32 + j4 * 4 + i] = (uint8_t)(w >> (8 * i));
+          }
+        }
+      }
+    }
+  }
+}
 
-// Shared-memory bytes finish_source_major needs for a batch of n_b sources.
-__host__ __device__ inline size_t transpose_smem_bytes(int n_b, int db, int words) {
-  const size_t rs = (size_t)n_b * db + (db == 1 ? 1 : 2);
-  return (((size_t)kTileV * rs + 15) & ~(size_t)15) + (size_t)kTileV * words * 4;
+// Any depth width and plane count (two-byte depths): lane = vertex.
+template <int WORDS>
+__device__ void output_generic(const Params& p, const GroupBufs& gb, uint8_t* depth_vm,
+                               const int32_t* rows, int n_b, int P, const Team& t) {
+  const uint32_t inf = p.db == 1 ? 0xFFu : 0xFFFFu;
+  for (long long v = t.tid; v < p.V; v += t.nthreads) {
+#pragma unroll 1
+    for (int k = 0; k < WORDS && k * 32 < n_b; k++) {
+      const uint32_t st = gb.last[(size_t)v * WORDS + k];
+      const int js = min(32, n_b - k * 32);
+      for (int j = 0; j < js; j++) {
+        uint32_t d = inf;
+        if ((st >> j) & 1u) {
+          d = 0;
+          for (int b = 0; b < P; b++)
+            d |= ((gb.planes[(size_t)b * p.plane_stride + (size_t)v * WORDS + k] >> j) & 1u) << b;
+        }
+        uint8_t* dst = p.layout == 0
+                           ? p.out + ((size_t)rows[k * 32 + j] * (size_t)p.V + (size_t)v) * p.db
+                           : depth_vm + ((size_t)v * n_b + k * 32 + j) * p.db;
+        if (p.db == 1) *dst = (uint8_t)d;
+        else *reinterpret_cast<uint16_t*>(dst) = (uint16_t)d;
+      }
+    }
+  }
+}
+
+template <int WORDS, int NP>
+__device__ __forceinline__ void output_u8(const Params& p, const GroupBufs& gb, uint8_t* depth_vm,
+                                          const int32_t* rows, int n_b, const Team& t) {
+  if (p.layout == 0) output_sm_u8<WORDS, NP>(p, gb, rows, n_b, t);
+  else output_vm_u8<WORDS, NP>(p, gb, depth_vm, n_b, t);
 }
 
 template <int WORDS>
-__device__ void finish_source_major(const Params& p, const GroupBufs& gb,
-                                    const uint8_t* stage, int n_b, long long k0,
-                                    uint8_t* smem, const Team& t) {
-  const int db = p.db;
-  const int rb = n_b * db;                 // row bytes in the staging array
-  const int rs = rb + (db == 1 ? 1 : 2);   // odd word stride: no bank conflicts
-  uint32_t* sst = reinterpret_cast<uint32_t*>(smem + (((size_t)kTileV * rs + 15) & ~(size_t)15));
-  const long long ntiles = (p.V + kTileV - 1) / kTileV;
-  const bool vec_out = p.vec_out != 0;
-  for (long long tile = t.block; tile < ntiles; tile += t.nblocks) {
-    const long long v0 = tile * kTileV;
-    const int nv = (int)min((long long)kTileV, p.V - v0);
-    __syncthreads();
-    // The tile's rows are one contiguous run of nv*rb bytes (16-byte aligned:
-    // v0 is a multiple of 128 and the staging base is 256-byte aligned).
-    const uint8_t* src = stage + (size_t)v0 * rb;
-    const int tot = nv * rb;
-    const int nvec = tot >> 4;
-    for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
-      const uint4 x = __ldcs(reinterpret_cast<const uint4*>(src) + i);
-      const uint32_t wv[4] = {x.x, x.y, x.z, x.w};
-#pragma unroll
-      for (int b = 0; b < 16; b++) {
-        const int o = i * 16 + b, r = o / rb, c = o - r * rb;
-        smem[r * rs + c] = (uint8_t)(wv[b >> 2] >> (8 * (b & 3)));
-      }
-    }
-    for (int o = nvec * 16 + threadIdx.x; o < tot; o += blockDim.x) {
-      const int r = o / rb, c = o - r * rb;
-      smem[r * rs + c] = src[o];
-    }
-    for (int i = threadIdx.x; i < nv * WORDS; i += blockDim.x)
-      sst[i] = __ldcg(gb.last + (size_t)v0 * WORDS + i);
-    __syncthreads();
-    // item = (source j, quad of 4 vertices q)
-    const int nq = (nv + 3) / 4;
-    for (int i = threadIdx.x; i < n_b * nq; i += blockDim.x) {
-      const int j = i / nq, q = i - j * nq;
-      uint8_t* orow = p.out + (size_t)p.out_row[k0 + j] * (size_t)p.V * db;
-      const uint32_t bitw = (uint32_t)j >> 5, bit = 1u << (j & 31);
-      uint32_t val[4];
-#pragma unroll
-      for (int r4 = 0; r4 < 4; r4++) {
-        const int r = q * 4 + r4;
-        val[r4] = db == 1 ? 0xFFu : 0xFFFFu;
-        if (r < nv && (sst[r * WORDS + bitw] & bit))
-          val[r4] = db == 1 ? (uint32_t)smem[r * rs + j]
-                            : (uint32_t)(smem[r * rs + 2 * j] | (smem[r * rs + 2 * j + 1] << 8));
-      }
-      if (vec_out && q * 4 + 4 <= nv) {
-        if (db == 1) {
-          *reinterpret_cast<uint32_t*>(orow + v0 + q * 4) =
-              val[0] | (val[1] << 8) | (val[2] << 16) | (val[3] << 24);
-        } else {
-          *reinterpret_cast<uint2*>(orow + 2 * (v0 + q * 4)) =
-              make_uint2(val[0] | (val[1] << 16), val[2] | (val[3] << 16));
-        }
-      } else {
-        for (int r = q * 4; r < min(q * 4 + 4, nv); r++) {
-          if (db == 1) orow[v0 + r] = (uint8_t)val[r - q * 4];
-          else reinterpret_cast<uint16_t*>(orow)[v0 + r] = (uint16_t)val[r - q * 4];
-        }
-      }
+__device__ void output_phase(const Params& p, const GroupBufs& gb, uint8_t* depth_vm,
+                             const int32_t* rows, int n_b, int max_level, const Team& t) {
+  const int P = planes_for(max_level);
+  if (p.db == 1) {
+    switch (P) {
+      case 0: output_u8<WORDS, 0>(p, gb, depth_vm, rows, n_b, t); return;
+      case 1: output_u8<WORDS, 1>(p, gb, depth_vm, rows, n_b, t); return;
+      case 2: output_u8<WORDS, 2>(p, gb, depth_vm, rows, n_b, t); return;
+      case 3: output_u8<WORDS, 3>(p, gb, depth_vm, rows, n_b, t); return;
+      case 4: output_u8<WORDS, 4>(p, gb, depth_vm, rows, n_b, t); return;
+      default: break;
     }
   }
+  output_generic<WORDS>(p, gb, depth_vm, rows, n_b, P, t);
 }
 
 }  // namespace ibfs

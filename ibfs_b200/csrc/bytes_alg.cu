@@ -21,6 +21,9 @@
 struct ibfs_graph;
 extern "C" ibfs_status ibfs_graph_device_csr(const ibfs_graph* g, const int64_t** beg,
                                              const int32_t** col);
+namespace ibfs {
+const int32_t* graph_host_col(const ibfs_graph* g);
+}
 extern "C" ibfs_status ibfs_graph_info(const ibfs_graph* g, int64_t* V, int64_t* E,
                                        int64_t* max_degree);
 
@@ -124,14 +127,31 @@ extern "C" ibfs_status ibfs_bytes_alg(ibfs_graph* g, const void* depth_dev, int6
   ibfs_graph_device_csr(g, &beg, &col);
   ibfs_graph_info(g, &V, &E, nullptr);
   const int words = width / 32;
+  // the model scans neighbours in the caller's CSR order (the device copy is
+  // reordered hub-first), so upload that order for the measurement
+  int32_t* col_in = nullptr;
+  if (E > 0) {
+    if (cudaMalloc(&col_in, sizeof(int32_t) * (size_t)E) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return IBFS_ERR_OOM;
+    }
+    cudaMemcpy(col_in, graph_host_col(g), sizeof(int32_t) * (size_t)E, cudaMemcpyHostToDevice);
+    col = col_in;
+  }
   uint32_t* mask = nullptr;
   unsigned long long* acc = nullptr;
   unsigned* maxl = nullptr;
-  if (cudaMalloc(&mask, sizeof(uint32_t) * (size_t)V * words) != cudaSuccess) return IBFS_ERR_OOM;
+  if (cudaMalloc(&mask, sizeof(uint32_t) * (size_t)V * words) != cudaSuccess) {
+    cudaFree(col_in);
+    (void)cudaGetLastError();
+    return IBFS_ERR_OOM;
+  }
   if (cudaMalloc(&acc, sizeof(unsigned long long) * 2) != cudaSuccess ||
       cudaMalloc(&maxl, sizeof(unsigned)) != cudaSuccess) {
     cudaFree(mask);
     cudaFree(acc);
+    cudaFree(col_in);
+    (void)cudaGetLastError();
     return IBFS_ERR_OOM;
   }
   ibfs_status st = IBFS_OK;
@@ -155,6 +175,7 @@ extern "C" ibfs_status ibfs_bytes_alg(ibfs_graph* g, const void* depth_dev, int6
   cudaFree(mask);
   cudaFree(acc);
   cudaFree(maxl);
+  cudaFree(col_in);
   *bytes = total;
   return st;
 }

@@ -42,23 +42,23 @@ __device__ __forceinline__ Team make_team(int block, int nblocks) {
   return t;
 }
 
-__device__ __forceinline__ void zero_words(uint32_t* p, long long nwords, const Team& t) {
-  // nwords is a multiple of 4 and p 16-byte aligned (allocation padding)
-  uint4* q = reinterpret_cast<uint4*>(p);
-  const uint4 z = make_uint4(0, 0, 0, 0);
-  for (long long i = t.tid; i < nwords / 4; i += t.nthreads) __stcg(q + i, z);
-}
-
 __device__ __forceinline__ int depth_limit(int db) { return db == 1 ? 254 : 65534; }
 
-__device__ __forceinline__ uint8_t* batch_depth(const Params& p, const GroupBufs& gb, int b) {
-  return p.layout == 1 ? p.out + (size_t)b * (size_t)p.V * p.C * p.db : gb.stage;
+__device__ __forceinline__ uint8_t* batch_depth(const Params& p, int b) {
+  return p.layout == 1 ? p.out + (size_t)b * (size_t)p.V * p.C * p.db : nullptr;
+}
+
+// Output rows of batch b (source-major) into shared memory.
+__device__ __forceinline__ void load_rows(const Params& p, int b, int n_b, int32_t* s_rows) {
+  if (p.layout == 0)
+    for (int j = threadIdx.x; j < n_b; j += blockDim.x) s_rows[j] = p.out_row[(long long)b * p.C + j];
+  __syncthreads();
 }
 
 template <int WORDS>
 __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
-  extern __shared__ __align__(16) uint8_t dsmem[];
-  __shared__ int s_dir, s_stop, s_err;
+  __shared__ int s_dir, s_stop, s_err, s_maxl;
+  __shared__ int32_t s_rows[kMaxWords * 32];
   const int g = blockIdx.x / p.cpg;
   const Team t = make_team(blockIdx.x % p.cpg, p.cpg);
   const GroupBufs gb = p.groups[g];
@@ -67,7 +67,6 @@ __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
   const bool lead = (t.block == 0 && threadIdx.x == 0);
   bool withhold = p.withhold && t.block == 0 && g == 0;
   const long long vpad = (p.V + 31) & ~31LL;
-  const long long nchg_pad = (p.nchg + 3) & ~3LL;
 
 #define BARRIER()                                                   \
   do {                                                              \
@@ -78,10 +77,10 @@ __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
   for (int b = g; b < p.nbatches; b += p.G) {
     const long long k0 = (long long)b * p.C;
     const int n_b = (int)min((long long)p.C, p.n_total - k0);
-    uint8_t* depth = batch_depth(p, gb, b);
     zero_words(gb.last, vpad * WORDS, t);
     zero_words(gb.curr, vpad * WORDS, t);
-    zero_words(gb.chg, nchg_pad, t);
+    zero_words(gb.chg, 2 * p.chg_stride, t);
+    load_rows(p, b, n_b, s_rows);
     if (lead) {
       memset(&ctl->par[0], 0, sizeof(Par) * 2);
       memset(&ctl->qc[0][0], 0, sizeof(ctl->qc));
@@ -89,7 +88,7 @@ __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
     BARRIER();
     seed_phase<WORDS>(p, gb, p.src + k0, n_b, t);
     BARRIER();
-    inspect_phase<WORDS>(p, gb, &ctl->par[0], depth, n_b, 0, true, t);
+    inspect_phase<WORDS>(p, gb, &ctl->par[0], n_b, 0, true, t);
     BARRIER();
     int level = 0, cur_dir = kDirTD, max_level = 0, td = 0, bu = 0;
     unsigned long long m_u = (unsigned long long)p.E, teps = 0;
@@ -105,10 +104,10 @@ __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
         else if (changed == 0) stop = 1;
         else if (level + 1 > p.max_levels) { stop = 1; err = 3; }
         if (changed && !pr->range_err) max_level = level;
-        int nd = choose_dir(level + 1, cur_dir, p.switch_level, p.alpha, p.beta,
-                            changed, mf, m_u, p.V);
+        const int nd = choose_dir(level + 1, cur_dir, p.switch_level, p.alpha, p.beta,
+                                  changed, mf, m_u, p.V);
         if (t.block == 0) {
-          if (b < p.nbatches && level < p.lrec_cap) {
+          if (level < p.lrec_cap) {
             LevelRec r;
             r.batch = b; r.level = level; r.dir = level == 0 ? -1 : cur_dir; r.pad = 0;
             r.frontier = (long long)changed; r.frontier_edges = (long long)mf;
@@ -122,6 +121,7 @@ __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
         s_dir = nd;
         s_stop = stop;
         s_err = err;
+        s_maxl = max_level;
       }
       __syncthreads();
       const int stop = s_stop;
@@ -130,17 +130,18 @@ __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
       __syncthreads();
       if (stop) break;
       level++;
+      zero_plane_if_first(p, gb, level, t);
       if (cur_dir == kDirTD) {
         td++;
-        qbuild_phase(p, gb, ctl->qc[level & 1], t);
+        qbuild_phase(p, gb, level, ctl->qc[level & 1], t);
         BARRIER();
-        td_phase<WORDS>(p, gb, ctl->qc[level & 1], t);
+        td_phase<WORDS>(p, gb, level, ctl->qc[level & 1], t);
       } else {
         bu++;
-        bu_phase<WORDS>(p, gb, ctl->par[(level - 1) & 1].fmask, t);
+        bu_phase<WORDS>(p, gb, level, ctl->par[(level - 1) & 1].fmask, t);
       }
       BARRIER();
-      inspect_phase<WORDS>(p, gb, &ctl->par[level & 1], depth, n_b, level,
+      inspect_phase<WORDS>(p, gb, &ctl->par[level & 1], n_b, level,
                            level <= depth_limit(p.db), t);
       BARRIER();
     }
@@ -151,8 +152,7 @@ __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
       }
       return;
     }
-    if (p.layout == 1) finish_vertex_major<WORDS>(p, gb, depth, n_b, t);
-    else finish_source_major<WORDS>(p, gb, depth, n_b, k0, dsmem, t);
+    output_phase<WORDS>(p, gb, batch_depth(p, b), s_rows, n_b, s_maxl, t);
     if (lead) {
       BatchRec r;
       r.levels = level;
@@ -183,36 +183,34 @@ __global__ void __launch_bounds__(512) k_inspect(Params p, GroupBufs gb, int b, 
   const Team t = make_team(blockIdx.x, gridDim.x);
   const long long k0 = (long long)b * p.C;
   const int n_b = (int)min((long long)p.C, p.n_total - k0);
-  inspect_phase<WORDS>(p, gb, &gb.ctl->par[level & 1], batch_depth(p, gb, b), n_b, level,
-                       level <= depth_limit(p.db), t);
+  inspect_phase<WORDS>(p, gb, &gb.ctl->par[level & 1], n_b, level, level <= depth_limit(p.db), t);
 }
 
 __global__ void __launch_bounds__(512) k_qbuild(Params p, GroupBufs gb, int level) {
   const Team t = make_team(blockIdx.x, gridDim.x);
-  qbuild_phase(p, gb, gb.ctl->qc[level & 1], t);
+  qbuild_phase(p, gb, level, gb.ctl->qc[level & 1], t);
 }
 
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_td(Params p, GroupBufs gb, int level) {
   const Team t = make_team(blockIdx.x, gridDim.x);
-  td_phase<WORDS>(p, gb, gb.ctl->qc[level & 1], t);
+  td_phase<WORDS>(p, gb, level, gb.ctl->qc[level & 1], t);
 }
 
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_bu(Params p, GroupBufs gb, int level) {
   const Team t = make_team(blockIdx.x, gridDim.x);
-  bu_phase<WORDS>(p, gb, gb.ctl->par[(level - 1) & 1].fmask, t);
+  bu_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask, t);
 }
 
 template <int WORDS>
-__global__ void __launch_bounds__(512) k_finish(Params p, GroupBufs gb, int b) {
-  extern __shared__ __align__(16) uint8_t dsmem[];
+__global__ void __launch_bounds__(512) k_output(Params p, GroupBufs gb, int b, int max_level) {
+  __shared__ int32_t s_rows[kMaxWords * 32];
   const Team t = make_team(blockIdx.x, gridDim.x);
   const long long k0 = (long long)b * p.C;
   const int n_b = (int)min((long long)p.C, p.n_total - k0);
-  uint8_t* depth = batch_depth(p, gb, b);
-  if (p.layout == 1) finish_vertex_major<WORDS>(p, gb, depth, n_b, t);
-  else finish_source_major<WORDS>(p, gb, depth, n_b, k0, dsmem, t);
+  load_rows(p, b, n_b, s_rows);
+  output_phase<WORDS>(p, gb, batch_depth(p, b), s_rows, n_b, max_level, t);
 }
 
 // ---------------------------------------------------------------------------
@@ -282,10 +280,10 @@ struct PinBuf {
 };
 
 struct GroupMem {
-  DevBuf last, curr, chg, qs, qm, ql, ctl, stage;
+  DevBuf last, curr, chg, qs, qm, ql, ctl, planes;
   void release() {
     last.release(); curr.release(); chg.release(); qs.release();
-    qm.release(); ql.release(); ctl.release(); stage.release();
+    qm.release(); ql.release(); ctl.release(); planes.release();
   }
 };
 
@@ -343,12 +341,12 @@ static ibfs_status check_opts(const ibfs_opts* o) {
 
 // Per-group workspace bytes for (V, W, C, db).
 static size_t group_bytes(int64_t V, int64_t E, int words, int C, int db, int lrg, int chunk,
-                          bool stage) {
+                          bool /*unused*/) {
   const size_t vpad = (size_t)((V + 31) & ~31LL);
   const size_t nchg = (size_t)(((V + 31) / 32 + 3) & ~3LL);
   const size_t capl = (size_t)(E / std::max(chunk, 1) + std::min<int64_t>(V, E / std::max(lrg, 1)) + 16);
   size_t b = 2 * vpad * words * 4 + nchg * 4 + 2 * (size_t)V * 4 + capl * 8 + sizeof(Ctl);
-  if (stage) b += (size_t)V * C * db;
+  b += (size_t)(db == 1 ? 8 : 16) * vpad * words * 4 + nchg * 4;  // planes + 2nd bitmap
   return b;
 }
 
@@ -390,9 +388,9 @@ static cudaError_t launch_plain_seed(const Params& p, int grid, int threads, int
 }
 
 template <int WORDS>
-static cudaError_t launch_plain_finish(const Params& p, const GroupBufs& gb, int grid, int threads,
-                                       int b, size_t smem, cudaStream_t s) {
-  k_finish<WORDS><<<grid, threads, smem, s>>>(p, gb, b);
+static cudaError_t launch_plain_output(const Params& p, const GroupBufs& gb, int grid, int threads,
+                                       int b, int max_level, cudaStream_t s) {
+  k_output<WORDS><<<grid, threads, 0, s>>>(p, gb, b, max_level);
   return cudaGetLastError();
 }
 
@@ -401,15 +399,6 @@ static cudaError_t launch_plain_finish(const Params& p, const GroupBufs& gb, int
    : (words) == 2 ? fn<2>(__VA_ARGS__)                  \
    : (words) == 4 ? fn<4>(__VA_ARGS__)                  \
                   : fn<8>(__VA_ARGS__))
-
-template <int WORDS>
-static cudaError_t set_smem_attrs(size_t smem) {
-  cudaError_t e = cudaFuncSetAttribute(persistent_kernel<WORDS>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_finish<WORDS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)smem);
-}
 
 struct RunPlan {
   int words, C, nbatches, G, cpg, threads, grid, db;
@@ -420,7 +409,7 @@ struct RunPlan {
 // Allocate / reuse the workspace for G groups.
 static ibfs_status ensure_workspace(ibfs_graph* g, const RunPlan& rp, const ibfs_opts& o,
                                     int layout) {
-  const bool stage = layout == IBFS_LAYOUT_SOURCE_MAJOR;
+  (void)layout;
   const size_t vpad = (size_t)((g->V + 31) & ~31LL);
   const size_t nchg = (size_t)(((g->V + 31) / 32 + 3) & ~3LL);
   const int chunk = rp.threads * 4;
@@ -431,12 +420,13 @@ static ibfs_status ensure_workspace(ibfs_graph* g, const RunPlan& rp, const ibfs
     ibfs_status s;
     if ((s = m.last.ensure(vpad * rp.words * 4)) != IBFS_OK) return s;
     if ((s = m.curr.ensure(vpad * rp.words * 4)) != IBFS_OK) return s;
-    if ((s = m.chg.ensure(nchg * 4)) != IBFS_OK) return s;
+    if ((s = m.chg.ensure(2 * nchg * 4)) != IBFS_OK) return s;
+    if ((s = m.planes.ensure((size_t)(rp.db == 1 ? 8 : 16) * vpad * rp.words * 4)) != IBFS_OK)
+      return s;
     if ((s = m.qs.ensure((size_t)g->V * 4)) != IBFS_OK) return s;
     if ((s = m.qm.ensure((size_t)g->V * 4)) != IBFS_OK) return s;
     if ((s = m.ql.ensure(capl * 8)) != IBFS_OK) return s;
     if ((s = m.ctl.ensure(sizeof(Ctl))) != IBFS_OK) return s;
-    if (stage && (s = m.stage.ensure((size_t)g->V * rp.C * rp.db)) != IBFS_OK) return s;
   }
   return IBFS_OK;
 }
@@ -515,9 +505,41 @@ static ibfs_status upload_graph(ibfs_graph* g) {
   CU(cudaEventCreate(&g->ev1));
   CU(cudaMemcpyAsync(g->beg.p, g->h.beg.data(), sizeof(int64_t) * (size_t)(g->V + 1),
                      cudaMemcpyHostToDevice, g->stream));
-  if (g->E)
-    CU(cudaMemcpyAsync(g->col.p, g->h.col.data(), sizeof(int32_t) * (size_t)g->E,
+  if (g->E) {
+    // Device adjacency order: every list sorted by neighbour degree, highest
+    // first (ties by id).  Depths do not depend on the order; the bottom-up
+    // sweep stops at the first neighbours that cover the missing bits, and
+    // hubs carry the most bits earliest.  The host copy keeps the caller's
+    // order (GroupBy's "first hub in CSR order" and the byte model use it).
+    std::vector<int32_t> dcol;
+    try {
+      dcol.resize((size_t)g->E);
+    } catch (const std::bad_alloc&) {
+      return IBFS_ERR_OOM;
+    }
+    const int64_t* bg = g->h.beg.data();
+    const int32_t* cl = g->h.col.data();
+    int64_t maxd = 0;
+    for (int64_t v = 0; v < g->V; v++) maxd = std::max(maxd, bg[v + 1] - bg[v]);
+#pragma omp parallel
+    {
+      std::vector<uint64_t> key;
+#pragma omp for schedule(dynamic, 4096)
+      for (int64_t v = 0; v < g->V; v++) {
+        const int64_t b0 = bg[v], b1 = bg[v + 1];
+        key.resize((size_t)(b1 - b0));
+        for (int64_t e = b0; e < b1; e++) {
+          const int32_t u = cl[e];
+          key[e - b0] = ((uint64_t)(maxd - (bg[u + 1] - bg[u])) << 32) | (uint32_t)u;
+        }
+        std::sort(key.begin(), key.end());
+        for (int64_t e = b0; e < b1; e++) dcol[e] = (int32_t)(key[e - b0] & 0xFFFFFFFFu);
+      }
+    }
+    CU(cudaMemcpyAsync(g->col.p, dcol.data(), sizeof(int32_t) * (size_t)g->E,
                        cudaMemcpyHostToDevice, g->stream));
+    CU(cudaStreamSynchronize(g->stream));
+  }
   CU(cudaStreamSynchronize(g->stream));
   int64_t md = 0;
   for (int64_t v = 0; v < g->V; v++) md = std::max(md, g->h.beg[v + 1] - g->h.beg[v]);
@@ -734,9 +756,8 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   rp.threads = o.threads ? o.threads : 512;
   rp.db = db;
   rp.host_out = !(flags & IBFS_OUT_DEVICE);
-  rp.smem = layout == IBFS_LAYOUT_SOURCE_MAJOR ? transpose_smem_bytes(rp.C, db, rp.words) : 0;
+  rp.smem = 0;
   const bool persistent = o.mode == IBFS_MODE_PERSISTENT;
-  if (rp.smem > 0) CU(DISPATCH_WORDS(rp.words, set_smem_attrs, rp.smem));
   // grid sizing
   int occ = 0;
   CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, persistent_for(rp.words), rp.threads,
@@ -755,7 +776,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
       size_t freeb = 0, totb = 0;
       if (cudaMemGetInfo(&freeb, &totb) == cudaSuccess) {
         const size_t per = group_bytes(g->V, g->E, rp.words, rp.C, db, o.lrg_shed, rp.threads * 4,
-                                       layout == IBFS_LAYOUT_SOURCE_MAJOR);
+                                       false);
         const size_t budget = (size_t)(freeb * 0.5);
         G = (int)std::max<size_t>(1, std::min<size_t>((size_t)G, budget / std::max<size_t>(per, 1)));
       }
@@ -811,7 +832,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     hgb[i].qm = m.qm.as<int32_t>();
     hgb[i].ql = m.ql.as<int2>();
     hgb[i].ctl = m.ctl.as<Ctl>();
-    hgb[i].stage = layout == IBFS_LAYOUT_SOURCE_MAJOR ? m.stage.as<uint8_t>() : nullptr;
+    hgb[i].planes = m.planes.as<uint32_t>();
   }
   Params p;
   std::memset(&p, 0, sizeof(p));
@@ -820,6 +841,8 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   p.V = g->V;
   p.E = g->E;
   p.nchg = (g->V + 31) / 32;
+  p.chg_stride = (p.nchg + 3) & ~3LL;
+  p.plane_stride = (long long)((g->V + 31) & ~31LL) * rp.words;
   p.src = g->d_src.as<int32_t>();
   p.out_row = g->d_outrow.as<int32_t>();
   p.n_total = n;
@@ -844,7 +867,8 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   p.brec = g->d_brec.as<BatchRec>();
   p.lrec = g->d_lrec.as<LevelRec>();
   p.lrec_cap = kLrecCap;
-  p.vec_out = (g->V % 4 == 0) && ((reinterpret_cast<uintptr_t>(dout) & 7) == 0);
+  p.vec_out = (rp.C % 4 == 0) && ((reinterpret_cast<uintptr_t>(dout) & 3) == 0);
+  p.vec_sm = (g->V % 4 == 0) && ((reinterpret_cast<uintptr_t>(dout) & 3) == 0);
 
   int64_t launches = 0;
   const bool use_graph = persistent && o.use_graph && !o.debug_withhold;
@@ -940,7 +964,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     for (int b = 0; b < rp.nbatches; b++) {
       CU(cudaMemsetAsync(gb.last, 0, vpad * rp.words * 4, s));
       CU(cudaMemsetAsync(gb.curr, 0, vpad * rp.words * 4, s));
-      CU(cudaMemsetAsync(gb.chg, 0, nchg * 4, s));
+      CU(cudaMemsetAsync(gb.chg, 0, 2 * nchg * 4, s));
       CU(cudaMemsetAsync(gb.ctl, 0, sizeof(Ctl), s));
       CU(DISPATCH_WORDS(rp.words, launch_plain_seed, p, grid, thr, b, s));
       CU(DISPATCH_WORDS(rp.words, launch_plain_inspect, p, gb, grid, thr, b, 0, s));
@@ -968,6 +992,11 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
         if (stop) break;
         cur_dir = nd;
         level++;
+        if ((level & (level - 1)) == 0) {
+          const int pb = __builtin_ctz((unsigned)level);
+          CU(cudaMemsetAsync(gb.planes + (size_t)pb * p.plane_stride, 0,
+                             (size_t)p.plane_stride * 4, s));
+        }
         CU(cudaMemsetAsync(&gb.ctl->par[level & 1], 0, sizeof(Par), s));
         CU(cudaMemsetAsync(&gb.ctl->qc[level & 1][0], 0, sizeof(int32_t) * 4, s));
         CU(DISPATCH_WORDS(rp.words, launch_plain_level, p, gb, grid, thr, level, cur_dir, s));
@@ -982,7 +1011,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
         *range_hit = err == 3;
         return (ibfs_status)err;
       }
-      CU(DISPATCH_WORDS(rp.words, launch_plain_finish, p, gb, grid, thr, b, rp.smem, s));
+      CU(DISPATCH_WORDS(rp.words, launch_plain_output, p, gb, grid, thr, b, max_level, s));
       launches += 1;
     }
     CU(cudaEventRecord(g->ev1, s));
@@ -1071,4 +1100,8 @@ cudaError_t persistent_occupancy(int words, int threads, size_t smem, int* per_s
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, persistent_for(words), threads,
                                                        smem);
 }
+}  // namespace ibfs
+
+namespace ibfs {
+const int32_t* graph_host_col(const ibfs_graph* g) { return g->h.col.data(); }
 }  // namespace ibfs

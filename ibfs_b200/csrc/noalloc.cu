@@ -97,7 +97,8 @@ extern "C" ibfs_status ibfs_run_static_scratch(const int64_t* beg_dev, const int
   const size_t o_lrec = off; off = align256(off + sizeof(LevelRec) * kMaxBatches * kLrecCap);
   const size_t o_last = off; off = align256(off + vpad * words * 4);
   const size_t o_curr = off; off = align256(off + vpad * words * 4);
-  const size_t o_chg = off; off = align256(off + nchg * 4);
+  const size_t o_chg = off; off = align256(off + 2 * nchg * 4);
+  const size_t o_planes = off; off = align256(off + 8 * vpad * words * 4);
   const size_t o_qs = off; off = align256(off + (size_t)V * 4);
   const size_t o_qm = off; off = align256(off + (size_t)V * 4);
   const size_t o_ql = off; off = align256(off + capl * 8);
@@ -121,11 +122,11 @@ extern "C" ibfs_status ibfs_run_static_scratch(const int64_t* beg_dev, const int
   gb.last = reinterpret_cast<uint32_t*>(base + o_last);
   gb.curr = reinterpret_cast<uint32_t*>(base + o_curr);
   gb.chg = reinterpret_cast<uint32_t*>(base + o_chg);
+  gb.planes = reinterpret_cast<uint32_t*>(base + o_planes);
   gb.qs = reinterpret_cast<int32_t*>(base + o_qs);
   gb.qm = reinterpret_cast<int32_t*>(base + o_qm);
   gb.ql = reinterpret_cast<int2*>(base + o_ql);
   gb.ctl = reinterpret_cast<Ctl*>(base + o_ctl);
-  gb.stage = nullptr;
   // What must start at zero: the control block (barrier, error, counters)
   // and the batch records.  Status words and bitmap are cleared per batch by
   // the kernel itself.
@@ -145,6 +146,8 @@ extern "C" ibfs_status ibfs_run_static_scratch(const int64_t* beg_dev, const int
   p.V = V;
   p.E = E;
   p.nchg = (V + 31) / 32;
+  p.chg_stride = (long long)nchg;
+  p.plane_stride = (long long)vpad * words;
   p.src = src_dev;
   p.out_row = nullptr;
   p.n_total = n;
@@ -169,7 +172,8 @@ extern "C" ibfs_status ibfs_run_static_scratch(const int64_t* beg_dev, const int
   p.brec = reinterpret_cast<BatchRec*>(base + o_brec);
   p.lrec = reinterpret_cast<LevelRec*>(base + o_lrec);
   p.lrec_cap = kLrecCap;
-  p.vec_out = 0;
+  p.vec_out = ((reinterpret_cast<uintptr_t>(depth_dev) & 3) == 0) ? 1 : 0;
+  p.vec_sm = 0;
   NA_CU(launch_persistent_params(p, words, p.cpg, threads, 0, s));
 
   int err = 0;
