@@ -20,7 +20,9 @@ from .api import (  # noqa: F401
     gen_grid,
     gen_rmat,
     graph_reader,
+    groupby_csr,
     lib_path,
+    read_csr,
     read_src_v,
     report,
     sample_sources,

@@ -73,10 +73,12 @@ _SIGS = [
     ("ibfs_version", C.c_char_p, []),
     ("ibfs_graph_open", C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(_P)]),
     ("ibfs_graph_from_csr", C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_int, C.POINTER(_P)]),
+    ("ibfs_csr_read", C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_P), C.POINTER(_P), _I64P, _I64P]),
     ("ibfs_graph_info", C.c_int, [_P, _I64P, _I64P, _I64P]),
     ("ibfs_graph_device_csr", C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
     ("ibfs_graph_close", C.c_int, [_P]),
     ("ibfs_groupby", C.c_int, [_P, _P, C.c_int64, _P]),
+    ("ibfs_groupby_csr", C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
     ("ibfs_read_sources", C.c_int, [C.c_char_p, _P, C.c_int64, _I64P]),
     ("ibfs_write_sources", C.c_int, [C.c_char_p, _P, C.c_int64]),
     ("ibfs_opts_default", None, [C.POINTER(Opts)]),
@@ -190,6 +192,15 @@ def csr_from_edges(src: np.ndarray, dst: np.ndarray, V: int) -> tuple[np.ndarray
     return _take_csr(bp, cp, V, E.value)
 
 
+def read_csr(beg_path: str, csr_path: str) -> tuple[np.ndarray, np.ndarray]:
+    """Host read of the binary CSR pair (graph_reader, graph_reader.cuh:63-119)."""
+    bp, cp = C.c_void_p(), C.c_void_p()
+    V, E = C.c_int64(), C.c_int64()
+    _check(_lib().ibfs_csr_read(beg_path.encode(), csr_path.encode(), C.byref(bp), C.byref(cp),
+                                C.byref(V), C.byref(E)), "ibfs_csr_read")
+    return _take_csr(bp, cp, V.value, E.value)
+
+
 def write_csr(beg_path: str, csr_path: str, beg: np.ndarray, col: np.ndarray) -> None:
     beg = np.ascontiguousarray(beg, np.int64)
     col = np.ascontiguousarray(col, np.int32)
@@ -205,6 +216,17 @@ def sample_sources(beg: np.ndarray, col: np.ndarray, n: int, seed: int,
     _check(_lib().ibfs_sample_sources(_ptr(beg), _ptr(col), len(beg) - 1, n, seed,
                                       0 if giant_component else -1, _ptr(out)),
            "ibfs_sample_sources")
+    return out
+
+
+def groupby_csr(beg: np.ndarray, col: np.ndarray, src: np.ndarray) -> np.ndarray:
+    """GroupBy (GroupBy.cuh:19-84) on host CSR arrays."""
+    beg = np.ascontiguousarray(beg, np.int64)
+    col = np.ascontiguousarray(col, np.int32)
+    src = np.ascontiguousarray(src, np.int32)
+    out = np.zeros_like(src)
+    _check(_lib().ibfs_groupby_csr(_ptr(beg), _ptr(col), len(beg) - 1, _ptr(src), len(src),
+                                   _ptr(out)), "ibfs_groupby_csr")
     return out
 
 

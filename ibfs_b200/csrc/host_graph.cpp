@@ -396,6 +396,15 @@ extern "C" ibfs_status ibfs_gen_chung_lu(int64_t n, int64_t m, double gamma,
   return export_csr(h, beg, col, V, E);
 }
 
+extern "C" ibfs_status ibfs_csr_read(const char* beg_path, const char* csr_path, int64_t** beg,
+                                     int32_t** col, int64_t* V, int64_t* E) {
+  if (!beg || !col || !V || !E) return IBFS_ERR_INVALID_ARG;
+  HostCsr h;
+  ibfs_status s = load_csr_files(beg_path, csr_path, &h);
+  if (s != IBFS_OK) return s;
+  return export_csr(h, beg, col, V, E);
+}
+
 extern "C" ibfs_status ibfs_csr_from_edges(const int32_t* src,
                                            const int32_t* dst, int64_t m,
                                            int64_t V, int64_t** beg,
@@ -519,6 +528,16 @@ extern "C" ibfs_status ibfs_sample_sources(const int64_t* beg,
     std::swap(cand[i], cand[j]);
     out[i] = cand[i];
   }
+  return IBFS_OK;
+}
+
+extern "C" ibfs_status ibfs_groupby_csr(const int64_t* beg, const int32_t* col, int64_t V,
+                                        const int32_t* src, int64_t n, int32_t* out) {
+  if (!beg || (!col && beg[V] > 0) || V <= 0 || n < 0 || (n > 0 && (!src || !out)))
+    return IBFS_ERR_INVALID_ARG;
+  for (int64_t i = 0; i < n; i++)
+    if (src[i] < 0 || src[i] >= V) return IBFS_ERR_RANGE;
+  groupby_host(beg, col, V, src, n, out);
   return IBFS_OK;
 }
 

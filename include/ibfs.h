@@ -9,10 +9,12 @@
  *
  * Reference interfaces each entry point replaces (file:line in iBFS):
  *   ibfs_graph_open        graph_reader::graph_reader      graph_reader.cuh:63-119
+ *   ibfs_csr_read          graph_reader::graph_reader      graph_reader.cuh:63-119
  *                          (+ graph<>::alloc_array CSR upload allocator.cuh:3-80)
  *   ibfs_graph_from_csr    graph<>::graph + alloc_array    graph.cuh:246-283, allocator.cuh:18-45
  *   ibfs_graph_close       (none: the reference never frees, gpu_ibfs.cuh:100)
  *   ibfs_groupby           GroupBy                         GroupBy.cuh:6-115
+ *   ibfs_groupby_csr       GroupBy                         GroupBy.cuh:6-115
  *   ibfs_run               graph<>::bfs_gpu_coalescing_mem bfs_gpu_opt.cuh:182-262
  *                          -> ibfs()                       bfs_gpu_opt.cuh:39-177
  *   ibfs_read_sources      read_src_v                      graph.cuh:99-133
@@ -135,6 +137,11 @@ ibfs_status ibfs_graph_open(const char *beg_path, const char *csr_path,
 ibfs_status ibfs_graph_from_csr(const int64_t *beg_pos_host,
                                 const int32_t *col_host, int64_t V,
                                 int64_t E, int device, ibfs_graph **out);
+/* Host-only read of the same files (graph_reader, graph_reader.cuh:63-119,
+   with validation instead of asserts): beg int64[V+1], col int32[E],
+   malloc'ed by the library (free with ibfs_free). */
+ibfs_status ibfs_csr_read(const char *beg_path, const char *csr_path,
+                          int64_t **beg, int32_t **col, int64_t *V, int64_t *E);
 ibfs_status ibfs_graph_info(const ibfs_graph *g, int64_t *V, int64_t *E,
                             int64_t *max_degree);
 /* Device pointers of the resident CSR (beg int64[V+1], col int32[E]). */
@@ -146,6 +153,10 @@ ibfs_status ibfs_graph_close(ibfs_graph *g);
 /* GroupBy reorder (host, exact restatement of GroupBy.cuh:19-84). */
 ibfs_status ibfs_groupby(const ibfs_graph *g, const int32_t *src_host,
                          int64_t n, int32_t *out_host);
+/* GroupBy on host CSR arrays (no graph handle, no GPU). */
+ibfs_status ibfs_groupby_csr(const int64_t *beg_host, const int32_t *col_host,
+                             int64_t V, const int32_t *src_host, int64_t n,
+                             int32_t *out_host);
 /* read_src_v format: one decimal vertex id per line.  With ids == NULL only
    *n is set; otherwise up to cap ids are written. */
 ibfs_status ibfs_read_sources(const char *path, int32_t *ids, int64_t cap,

@@ -1,0 +1,22 @@
+#!/usr/bin/env bash
+# Build oracle/_ref/ref_harness from the reference's own sources, where they
+# lie (REF, default /root/reference).  Outputs go to oracle/_ref/ only.  The
+# reference's GPU code targets sm_35 and does not compile for sm_100a; the
+# headers are compiled here for sm_52 only so that their host functions can
+# run on the CPU -- no kernel of theirs is ever launched.
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${REF:-/root/reference}"
+OUT="$HERE/_ref"
+if [ ! -f "$REF/graph.h" ]; then
+  echo "reference sources not present; keeping any prebuilt $OUT"
+  exit 0
+fi
+mkdir -p "$OUT"
+if [ -x "$OUT/ref_harness" ] && [ "$OUT/ref_harness" -nt "$HERE/ref_harness.cu" ]; then
+  echo "up to date"
+  exit 0
+fi
+nvcc -arch=sm_52 -O2 -w -Wno-deprecated-gpu-targets -I"$REF" -Xcompiler -fopenmp \
+  "$HERE/ref_harness.cu" -o "$OUT/ref_harness"
+echo "built $OUT/ref_harness"
