@@ -12,6 +12,7 @@ from .api import (  # noqa: F401
     GroupBy,
     IbfsError,
     Opts,
+    Server,
     Stats,
     csr_from_edges,
     default_opts,

@@ -62,6 +62,24 @@ class Stats(C.Structure):
     ]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("run", Opts), ("arena_bytes", C.c_int64), ("max_waiting", C.c_int32),
+                ("round_batches", C.c_int32), ("max_wait_us", C.c_int32), ("groupby", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
+
+
+class QueryInfo(C.Structure):
+    _fields_ = [("n_sources", C.c_int64), ("latency_ms", C.c_double), ("queue_ms", C.c_double),
+                ("status", C.c_int32), ("depth_bytes", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("refused", C.c_int64),
+                ("rounds", C.c_int64), ("sources", C.c_int64), ("traversed_edges", C.c_int64),
+                ("busy_ms", C.c_double), ("wall_ms", C.c_double), ("arena_rows", C.c_int64),
+                ("arena_rows_used", C.c_int64)]
+
+
 _LIB = None
 
 # (name, restype, argtypes) for every entry point of include/ibfs.h
@@ -86,9 +104,20 @@ _SIGS = [
                            C.POINTER(Stats)]),
     ("ibfs_set_stream", C.c_int, [_P, _P]),
     ("ibfs_teps", C.c_int, [_P, _P, C.c_int64, C.c_int32, _I64P]),
+    ("ibfs_autotune", C.c_int, [_P, _P, C.c_int64, C.POINTER(Opts), C.c_int32, C.POINTER(Opts),
+                                C.POINTER(C.c_double), C.c_char_p, C.c_int32]),
     ("ibfs_bytes_alg", C.c_int, [_P, _P, C.c_int64, C.c_int32, C.c_int32, _I64P]),
     ("ibfs_run_static_scratch", C.c_int, [_P, _P, C.c_int64, C.c_int64, _P, C.c_int64, C.c_int32,
                                           _P, _P, _I64P]),
+    ("ibfs_server_opts_default", None, [C.POINTER(ServerOpts)]),
+    ("ibfs_server_create", C.c_int, [_P, C.POINTER(ServerOpts), C.POINTER(_P)]),
+    ("ibfs_server_submit", C.c_int, [_P, _P, C.c_int64, C.POINTER(C.c_uint64)]),
+    ("ibfs_server_poll", C.c_int, [_P, C.c_uint64, _P, C.c_uint32, C.POINTER(C.c_int32),
+                                   C.POINTER(QueryInfo)]),
+    ("ibfs_server_wait", C.c_int, [_P, C.c_uint64, C.c_int32, _P, C.c_uint32,
+                                   C.POINTER(QueryInfo)]),
+    ("ibfs_server_stats_get", C.c_int, [_P, C.POINTER(ServerStats)]),
+    ("ibfs_server_destroy", C.c_int, [_P]),
     ("ibfs_gen_rmat", C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                 C.c_uint64, C.POINTER(_P), C.POINTER(_P), _I64P, _I64P]),
     ("ibfs_gen_grid", C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_uint64,
@@ -319,6 +348,20 @@ class Graph:
                                 C.byref(e)), "ibfs_teps")
         return e.value
 
+    def autotune(self, src, base: Opts | None = None, reps: int = 2) -> tuple[Opts, float, list]:
+        """Tune the options on this graph with a sample of sources."""
+        import json
+
+        src = np.ascontiguousarray(src, np.int32)
+        best = Opts()
+        g = C.c_double()
+        buf = C.create_string_buffer(1 << 16)
+        _check(_lib().ibfs_autotune(self._h, _ptr(src), len(src),
+                                    C.byref(base) if base is not None else None, reps,
+                                    C.byref(best), C.byref(g), buf, len(buf)), "ibfs_autotune")
+        log = [json.loads(ln) for ln in buf.value.decode().split("\n") if ln.strip()]
+        return best, g.value, log
+
     def bytes_alg(self, depth_dev_ptr: int, n: int, depth_bytes: int, width: int) -> int:
         b = C.c_int64()
         _check(_lib().ibfs_bytes_alg(self._h, C.c_void_p(depth_dev_ptr), n, depth_bytes, width,
@@ -384,6 +427,86 @@ def _levels(recs, st: Stats) -> list:
     return [dict(batch=recs[i].batch, level=recs[i].level, dir=recs[i].dir,
                  frontier=recs[i].frontier, frontier_edges=recs[i].frontier_edges)
             for i in range(st.levels_len)]
+
+
+class Server:
+    """Continuous-batching query server on a resident graph (ibfs_server_*)."""
+
+    def __init__(self, graph: "Graph", **kw):
+        so = ServerOpts()
+        _lib().ibfs_server_opts_default(C.byref(so))
+        for k, v in kw.items():
+            if hasattr(so, k):
+                setattr(so, k, v)
+            elif hasattr(so.run, k):
+                setattr(so.run, k, v)
+            else:
+                raise TypeError(f"unknown server option {k}")
+        self.graph = graph
+        self.V = graph.V
+        self.db = 2 if so.run.depth_bytes == 2 else 1
+        h = C.c_void_p()
+        _check(_lib().ibfs_server_create(graph.handle, C.byref(so), C.byref(h)),
+               "ibfs_server_create")
+        self._h = h
+
+    def submit(self, src) -> int:
+        src = np.ascontiguousarray(src, np.int32)
+        qid = C.c_uint64()
+        _check(_lib().ibfs_server_submit(self._h, _ptr(src), len(src), C.byref(qid)),
+               "ibfs_server_submit")
+        return qid.value
+
+    def try_submit(self, src) -> int | None:
+        """Submit, or None when admission refuses (IBFS_ERR_BUSY)."""
+        src = np.ascontiguousarray(src, np.int32)
+        qid = C.c_uint64()
+        st = _lib().ibfs_server_submit(self._h, _ptr(src), len(src), C.byref(qid))
+        if st == 9:
+            return None
+        _check(st, "ibfs_server_submit")
+        return qid.value
+
+    def poll(self, qid: int, n: int, want_depth: bool = True):
+        """(done, depth or None, info dict)"""
+        done = C.c_int32()
+        info = QueryInfo()
+        buf = np.empty((n, self.V), np.uint8 if self.db == 1 else np.uint16) if want_depth \
+            else None
+        _check(_lib().ibfs_server_poll(self._h, qid, _ptr(buf) if buf is not None else None, 0,
+                                       C.byref(done), C.byref(info)), "ibfs_server_poll")
+        if not done.value:
+            return False, None, None
+        return True, buf, _info(info)
+
+    def wait(self, qid: int, n: int, timeout_ms: int = 60000, want_depth: bool = True):
+        info = QueryInfo()
+        buf = np.empty((n, self.V), np.uint8 if self.db == 1 else np.uint16) if want_depth \
+            else None
+        _check(_lib().ibfs_server_wait(self._h, qid, timeout_ms,
+                                       _ptr(buf) if buf is not None else None, 0, C.byref(info)),
+               "ibfs_server_wait")
+        return buf, _info(info)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(_lib().ibfs_server_stats_get(self._h, C.byref(st)), "ibfs_server_stats_get")
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            _lib().ibfs_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def _info(info: QueryInfo) -> dict:
+    return {k: getattr(info, k) for k, _ in QueryInfo._fields_}
 
 
 # Reference-named aliases ----------------------------------------------------

@@ -711,7 +711,7 @@ static void order_sources(const ibfs_graph* g, const int32_t* src, int64_t n, bo
 
 static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const ibfs_opts& o,
                             int db, void* depth_out, int32_t layout, uint32_t flags,
-                            ibfs_stats* st, bool* range_hit);
+                            ibfs_stats* st, bool* range_hit, const int32_t* rows_in = nullptr);
 
 extern "C" ibfs_status ibfs_run(ibfs_graph* g, const int32_t* src_host, int64_t n,
                                 const ibfs_opts* opts, void* depth_out, int32_t layout,
@@ -745,7 +745,7 @@ extern "C" ibfs_status ibfs_run(ibfs_graph* g, const int32_t* src_host, int64_t 
 
 static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const ibfs_opts& o,
                             int db, void* depth_out, int32_t layout, uint32_t flags,
-                            ibfs_stats* st, bool* range_hit) {
+                            ibfs_stats* st, bool* range_hit, const int32_t* rows_in) {
   *range_hit = false;
   cudaStream_t s = g->stream;
   RunPlan rp;
@@ -794,7 +794,12 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   if (es != IBFS_OK) return es;
   // ordered sources and their output rows
   std::vector<int32_t> ord, row;
-  order_sources(g, src, n, o.groupby != 0, &ord, &row);
+  if (rows_in) {
+    ord.assign(src, src + n);  // already batched by the caller (the server)
+    row.assign(rows_in, rows_in + n);
+  } else {
+    order_sources(g, src, n, o.groupby != 0, &ord, &row);
+  }
   ibfs_status bs;
   if ((bs = g->h_src.ensure(sizeof(int32_t) * n)) != IBFS_OK) return bs;
   if ((bs = g->h_outrow.ensure(sizeof(int32_t) * n)) != IBFS_OK) return bs;
@@ -1104,4 +1109,22 @@ cudaError_t persistent_occupancy(int words, int threads, size_t smem, int* per_s
 
 namespace ibfs {
 const int32_t* graph_host_col(const ibfs_graph* g) { return g->h.col.data(); }
+}  // namespace ibfs
+
+namespace ibfs {
+// Run already-ordered sources whose depths go to explicit rows of a device
+// array (source-major, V depths per row): the server's rounds.
+ibfs_status run_rows(ibfs_graph* g, const int32_t* src, const int32_t* rows, int64_t n,
+                     const ibfs_opts& o, void* dev_out, ibfs_stats* st) {
+  if (!g || !src || !rows || n <= 0 || !dev_out) return IBFS_ERR_INVALID_ARG;
+  ibfs_status s = check_opts(&o);
+  if (s != IBFS_OK) return s;
+  std::lock_guard<std::mutex> lk(g->mu);
+  if (cudaSetDevice(g->device) != cudaSuccess) return IBFS_ERR_CUDA;
+  bool range_hit = false;
+  return run_once(g, src, n, o, o.depth_bytes ? o.depth_bytes : 1, dev_out,
+                  IBFS_LAYOUT_SOURCE_MAJOR, IBFS_OUT_DEVICE, st, &range_hit, rows);
+}
+int graph_device(const ibfs_graph* g) { return g->device; }
+const int64_t* graph_host_beg(const ibfs_graph* g) { return g->h.beg.data(); }
 }  // namespace ibfs

@@ -50,3 +50,12 @@ cudaError_t launch_persistent_params(const Params& p, int words, int grid, int t
                                      size_t smem, cudaStream_t s);
 cudaError_t persistent_occupancy(int words, int threads, size_t smem, int* per_sm);
 }  // namespace ibfs
+
+namespace ibfs {
+// engine.cu: already-ordered sources into explicit rows of a device array.
+ibfs_status run_rows(ibfs_graph* g, const int32_t* src, const int32_t* rows, int64_t n,
+                     const ibfs_opts& o, void* dev_out, ibfs_stats* st);
+int graph_device(const ibfs_graph* g);
+const int64_t* graph_host_beg(const ibfs_graph* g);
+const int32_t* graph_host_col(const ibfs_graph* g);
+}  // namespace ibfs

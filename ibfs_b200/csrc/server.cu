@@ -1,0 +1,395 @@
+// server.cu -- continuous-batching BFS query server over a resident graph.
+//
+// Queries of 1..N sources arrive at any time (ibfs_server_submit, thread
+// safe).  A worker thread
+//   1. admits queries in arrival order as device memory allows: each query
+//      owns k contiguous rows of V depths in a device arena (its per-query
+//      state; a query that can never fit is refused, a full waiting queue
+//      refuses with IBFS_ERR_BUSY);
+//   2. takes the admitted, not yet traversed sources of ALL queries (first
+//      come first served, up to one round of `round_batches` batches of
+//      `concurrent` sources), regroups them with GroupBy (GroupBy.cuh:19-84)
+//      so sources that share hubs share a batch, and runs them as one
+//      persistent launch whose depths land directly in each query's rows;
+//   3. completes a query when its last source has been traversed.
+// Sources that arrive while a round is on the GPU join the next round, and
+// one round mixes sources of many queries: their work overlaps on the device.
+// A query's depths are the same alone or in a mix because every source owns
+// its own status bit and output row.  Results stay in the arena until the
+// client polls them (host or device copy), which frees the rows and admits
+// waiting queries.
+//
+// The reference has no serving path (it runs one fixed source list,
+// bfs_gpu_opt.cuh:182-262); this is the serving pattern added beside it.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace {
+
+using clock_t_ = std::chrono::steady_clock;
+
+double ms_between(clock_t_::time_point a, clock_t_::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+struct Query {
+  std::vector<int32_t> src;
+  int64_t row0 = -1;  // first arena row, -1 until admitted
+  int64_t remaining = 0;
+  int32_t status = IBFS_OK;
+  bool done = false;
+  bool started = false;
+  clock_t_::time_point t_submit, t_start, t_done;
+};
+
+// First-fit allocator of contiguous row ranges.
+struct RowArena {
+  std::map<int64_t, int64_t> free_;  // start -> length
+  int64_t rows = 0, used = 0;
+  void init(int64_t r) {
+    rows = r;
+    used = 0;
+    free_.clear();
+    if (r > 0) free_[0] = r;
+  }
+  int64_t alloc(int64_t k) {
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= k) {
+        const int64_t s = it->first, len = it->second;
+        free_.erase(it);
+        if (len > k) free_[s + k] = len - k;
+        used += k;
+        return s;
+      }
+    }
+    return -1;
+  }
+  void release(int64_t s, int64_t k) {
+    used -= k;
+    auto it = free_.emplace(s, k).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+};
+
+}  // namespace
+
+struct ibfs_server {
+  ibfs_graph* g = nullptr;
+  ibfs_server_opts so;
+  int64_t V = 0;
+  int db = 1;
+  int64_t C = 128;
+  void* arena = nullptr;
+  RowArena rows;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::thread worker;
+  bool stop = false;
+  uint64_t next_id = 1;
+  std::unordered_map<uint64_t, Query> q;
+  std::deque<uint64_t> waiting;                          // not admitted yet
+  std::deque<std::pair<uint64_t, int64_t>> pending;      // admitted sources (query, index)
+  clock_t_::time_point t_create;
+  ibfs_server_stats st;
+};
+
+using namespace ibfs;
+
+static void admit_locked(ibfs_server* s) {
+  while (!s->waiting.empty()) {
+    const uint64_t id = s->waiting.front();
+    Query& qq = s->q[id];
+    const int64_t r = s->rows.alloc((int64_t)qq.src.size());
+    if (r < 0) break;  // head of line waits for memory (first come, first served)
+    qq.row0 = r;
+    for (int64_t i = 0; i < (int64_t)qq.src.size(); i++) s->pending.emplace_back(id, i);
+    s->waiting.pop_front();
+  }
+}
+
+static void worker_loop(ibfs_server* s) {
+  cudaSetDevice(graph_device(s->g));
+  const int64_t cap = (int64_t)std::max(1, s->so.round_batches) * s->C;
+  std::vector<int32_t> src, rows, ord, ordrows;
+  std::vector<std::pair<uint64_t, int64_t>> taken;
+  for (;;) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    admit_locked(s);
+    if (s->stop) break;
+    if (s->pending.empty()) {
+      s->cv.wait_for(lk, std::chrono::milliseconds(20));
+      continue;
+    }
+    if ((int64_t)s->pending.size() < cap && s->waiting.empty()) {
+      // a partial round may wait a little for more sources
+      const auto oldest = s->q[s->pending.front().first].t_submit;
+      const auto deadline = oldest + std::chrono::microseconds(s->so.max_wait_us);
+      if (clock_t_::now() < deadline) {
+        s->cv.wait_until(lk, deadline);
+        continue;
+      }
+    }
+    const int64_t n = std::min<int64_t>(cap, (int64_t)s->pending.size());
+    taken.assign(s->pending.begin(), s->pending.begin() + n);
+    s->pending.erase(s->pending.begin(), s->pending.begin() + n);
+    src.resize((size_t)n);
+    rows.resize((size_t)n);
+    const auto now = clock_t_::now();
+    for (int64_t i = 0; i < n; i++) {
+      Query& qq = s->q[taken[i].first];
+      src[i] = qq.src[taken[i].second];
+      rows[i] = (int32_t)(qq.row0 + taken[i].second);
+      if (!qq.started) {
+        qq.started = true;
+        qq.t_start = now;
+      }
+    }
+    lk.unlock();
+    // Regroup the round's sources with GroupBy; rows travel with them.
+    ord.resize((size_t)n);
+    ordrows.resize((size_t)n);
+    if (s->so.groupby) {
+      std::vector<int64_t> idx((size_t)n);
+      for (int64_t i = 0; i < n; i++) idx[i] = i;
+      std::vector<int32_t> tmp((size_t)n);
+      groupby_host(graph_host_beg(s->g), graph_host_col(s->g), s->V, src.data(), n, tmp.data());
+      // map the reordered ids back to positions, stable for repeated ids
+      std::vector<std::pair<int32_t, int64_t>> a((size_t)n), b((size_t)n);
+      for (int64_t i = 0; i < n; i++) a[i] = {src[i], i};
+      for (int64_t k = 0; k < n; k++) b[k] = {tmp[k], k};
+      std::stable_sort(a.begin(), a.end(),
+                       [](const auto& x, const auto& y) { return x.first < y.first; });
+      std::stable_sort(b.begin(), b.end(),
+                       [](const auto& x, const auto& y) { return x.first < y.first; });
+      for (int64_t i = 0; i < n; i++) {
+        ord[b[i].second] = src[a[i].second];
+        ordrows[b[i].second] = rows[a[i].second];
+      }
+    } else {
+      ord = src;
+      ordrows = rows;
+    }
+    ibfs_stats rs;
+    std::memset(&rs, 0, sizeof(rs));
+    ibfs_opts ro = s->so.run;
+    ro.depth_bytes = s->db;
+    ro.mode = IBFS_MODE_PERSISTENT;
+    ro.use_graph = 0;
+    ro.groupby = 0;
+    const ibfs_status rc = run_rows(s->g, ord.data(), ordrows.data(), n, ro, s->arena, &rs);
+    lk.lock();
+    const auto t_end = clock_t_::now();
+    s->st.rounds++;
+    s->st.sources += n;
+    if (rc == IBFS_OK) {
+      s->st.traversed_edges += rs.traversed_edges;
+      s->st.busy_ms += rs.device_ms;
+    }
+    for (int64_t i = 0; i < n; i++) {
+      Query& qq = s->q[taken[i].first];
+      if (rc != IBFS_OK) qq.status = rc;
+      if (--qq.remaining == 0) {
+        qq.done = true;
+        qq.t_done = t_end;
+        s->st.completed++;
+      }
+    }
+    lk.unlock();
+    s->cv.notify_all();
+  }
+}
+
+extern "C" void ibfs_server_opts_default(ibfs_server_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  ibfs_opts_default(&o->run);
+  o->arena_bytes = 0;
+  o->max_waiting = 4096;
+  o->round_batches = 4;
+  o->max_wait_us = 200;
+  o->groupby = 1;
+}
+
+extern "C" ibfs_status ibfs_server_create(ibfs_graph* g, const ibfs_server_opts* opts,
+                                          ibfs_server** out) {
+  if (!g || !out) return IBFS_ERR_INVALID_ARG;
+  *out = nullptr;
+  ibfs_server* s = new (std::nothrow) ibfs_server();
+  if (!s) return IBFS_ERR_OOM;
+  if (opts) s->so = *opts;
+  else ibfs_server_opts_default(&s->so);
+  if (s->so.max_waiting <= 0) s->so.max_waiting = 4096;
+  if (s->so.round_batches <= 0) s->so.round_batches = 4;
+  if (s->so.max_wait_us < 0) s->so.max_wait_us = 0;
+  s->g = g;
+  int64_t E = 0;
+  ibfs_graph_info(g, &s->V, &E, nullptr);
+  s->db = s->so.run.depth_bytes == 2 ? 2 : 1;
+  s->C = s->so.run.concurrent ? s->so.run.concurrent : s->so.run.width;
+  if (s->C <= 0 || s->C > 256) {
+    delete s;
+    return IBFS_ERR_INVALID_ARG;
+  }
+  cudaSetDevice(graph_device(g));
+  size_t bytes = (size_t)s->so.arena_bytes;
+  if (bytes == 0) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      (void)cudaGetLastError();
+      delete s;
+      return IBFS_ERR_CUDA;
+    }
+    bytes = fr / 4;
+  }
+  const size_t row_bytes = (size_t)s->V * s->db;
+  const int64_t nrows = (int64_t)(bytes / row_bytes);
+  if (nrows < 1) {
+    delete s;
+    return IBFS_ERR_OOM;
+  }
+  if (cudaMalloc(&s->arena, (size_t)nrows * row_bytes) != cudaSuccess) {
+    (void)cudaGetLastError();
+    delete s;
+    return IBFS_ERR_OOM;
+  }
+  s->rows.init(nrows);
+  std::memset(&s->st, 0, sizeof(s->st));
+  s->st.arena_rows = nrows;
+  s->t_create = clock_t_::now();
+  try {
+    s->worker = std::thread(worker_loop, s);
+  } catch (...) {
+    cudaFree(s->arena);
+    delete s;
+    return IBFS_ERR_OOM;
+  }
+  *out = s;
+  return IBFS_OK;
+}
+
+extern "C" ibfs_status ibfs_server_submit(ibfs_server* s, const int32_t* src, int64_t n,
+                                          uint64_t* qid) {
+  if (!s || !src || n <= 0 || !qid) return IBFS_ERR_INVALID_ARG;
+  for (int64_t i = 0; i < n; i++)
+    if (src[i] < 0 || src[i] >= s->V) return IBFS_ERR_RANGE;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (n > s->rows.rows) {
+    s->st.refused++;
+    return IBFS_ERR_RANGE;  // can never fit the arena
+  }
+  if ((int64_t)s->waiting.size() >= s->so.max_waiting) {
+    s->st.refused++;
+    return IBFS_ERR_BUSY;
+  }
+  const uint64_t id = s->next_id++;
+  Query& qq = s->q[id];
+  qq.src.assign(src, src + n);
+  qq.remaining = n;
+  qq.t_submit = clock_t_::now();
+  s->waiting.push_back(id);
+  s->st.submitted++;
+  *qid = id;
+  s->cv.notify_all();
+  return IBFS_OK;
+}
+
+static ibfs_status collect_locked(ibfs_server* s, uint64_t qid, void* out, uint32_t flags,
+                                  ibfs_query_info* info) {
+  auto it = s->q.find(qid);
+  Query& qq = it->second;
+  if (info) {
+    info->n_sources = (int64_t)qq.src.size();
+    info->latency_ms = ms_between(qq.t_submit, qq.t_done);
+    info->queue_ms = qq.started ? ms_between(qq.t_submit, qq.t_start) : 0.0;
+    info->status = qq.status;
+    info->depth_bytes = s->db;
+  }
+  ibfs_status rc = (ibfs_status)qq.status;
+  if (rc == IBFS_OK && out) {
+    const size_t bytes = qq.src.size() * (size_t)s->V * s->db;
+    const uint8_t* from = static_cast<uint8_t*>(s->arena) + (size_t)qq.row0 * s->V * s->db;
+    const cudaError_t e = cudaMemcpy(out, from, bytes,
+                                     (flags & IBFS_OUT_DEVICE) ? cudaMemcpyDeviceToDevice
+                                                               : cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      rc = IBFS_ERR_CUDA;
+    }
+  }
+  s->rows.release(qq.row0, (int64_t)qq.src.size());
+  s->q.erase(it);
+  s->cv.notify_all();  // rows freed: the worker may admit waiting queries
+  return rc;
+}
+
+extern "C" ibfs_status ibfs_server_poll(ibfs_server* s, uint64_t qid, void* out, uint32_t flags,
+                                        int32_t* done, ibfs_query_info* info) {
+  if (!s || !done) return IBFS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->q.find(qid);
+  if (it == s->q.end()) return IBFS_ERR_NOT_FOUND;
+  *done = it->second.done ? 1 : 0;
+  if (!it->second.done) return IBFS_OK;
+  return collect_locked(s, qid, out, flags, info);
+}
+
+extern "C" ibfs_status ibfs_server_wait(ibfs_server* s, uint64_t qid, int32_t timeout_ms,
+                                        void* out, uint32_t flags, ibfs_query_info* info) {
+  if (!s) return IBFS_ERR_INVALID_ARG;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->q.find(qid);
+  if (it == s->q.end()) return IBFS_ERR_NOT_FOUND;
+  const auto deadline = clock_t_::now() + std::chrono::milliseconds(timeout_ms);
+  while (!s->q[qid].done) {
+    if (s->cv.wait_until(lk, deadline) == std::cv_status::timeout && !s->q[qid].done)
+      return IBFS_ERR_TIMEOUT;
+  }
+  return collect_locked(s, qid, out, flags, info);
+}
+
+extern "C" ibfs_status ibfs_server_stats_get(ibfs_server* s, ibfs_server_stats* out) {
+  if (!s || !out) return IBFS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  *out = s->st;
+  out->wall_ms = ms_between(s->t_create, clock_t_::now());
+  out->arena_rows_used = s->rows.used;
+  return IBFS_OK;
+}
+
+extern "C" ibfs_status ibfs_server_destroy(ibfs_server* s) {
+  if (!s) return IBFS_ERR_INVALID_ARG;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  cudaSetDevice(graph_device(s->g));
+  if (s->arena) cudaFree(s->arena);
+  delete s;
+  return IBFS_OK;
+}

@@ -174,6 +174,60 @@ ibfs_status ibfs_run(ibfs_graph *g, const int32_t *src_host, int64_t n,
 /* Launch on a caller stream (cudaStream_t) instead of the handle's own. */
 ibfs_status ibfs_set_stream(ibfs_graph *g, void *cuda_stream);
 
+/* ---- serving (no counterpart in the reference, which runs one fixed
+   source list, bfs_gpu_opt.cuh:182-262) --------------------------------- */
+typedef struct ibfs_server ibfs_server;
+typedef struct ibfs_server_opts {
+    ibfs_opts run;           /* traversal options of every round               */
+    int64_t arena_bytes;     /* device memory for per-query depth rows
+                                (0: a quarter of the free device memory)       */
+    int32_t max_waiting;     /* queued submissions beyond this: IBFS_ERR_BUSY  */
+    int32_t round_batches;   /* batches of `concurrent` sources per round      */
+    int32_t max_wait_us;     /* a partial round waits this long for sources    */
+    int32_t groupby;         /* regroup each round's sources with GroupBy      */
+    int32_t reserved[6];
+} ibfs_server_opts;
+typedef struct ibfs_query_info {
+    int64_t n_sources;
+    double latency_ms;       /* submission to depths complete on the device     */
+    double queue_ms;         /* submission to the first round that included it  */
+    int32_t status;          /* ibfs_status of the query                        */
+    int32_t depth_bytes;
+} ibfs_query_info;
+typedef struct ibfs_server_stats {
+    int64_t submitted, completed, refused, rounds, sources, traversed_edges;
+    double busy_ms;          /* device time of all rounds                       */
+    double wall_ms;          /* since creation                                  */
+    int64_t arena_rows, arena_rows_used;
+} ibfs_server_stats;
+void ibfs_server_opts_default(ibfs_server_opts *o);
+/* Start a server (worker thread) on a resident graph. */
+ibfs_status ibfs_server_create(ibfs_graph *g, const ibfs_server_opts *o,
+                               ibfs_server **out);
+/* Queue a query of n sources; thread safe.  IBFS_ERR_BUSY when the waiting
+   queue is full, IBFS_ERR_RANGE when n rows can never fit the arena. */
+ibfs_status ibfs_server_submit(ibfs_server *s, const int32_t *src_host, int64_t n,
+                               uint64_t *qid);
+/* Non-blocking: *done = 1 and depths [n][V] copied to depth_out (host, or
+   device with IBFS_OUT_DEVICE; NULL to discard) once complete; the query is
+   then forgotten. */
+ibfs_status ibfs_server_poll(ibfs_server *s, uint64_t qid, void *depth_out,
+                             uint32_t flags, int32_t *done, ibfs_query_info *info);
+/* Blocking variant with a timeout (IBFS_ERR_TIMEOUT). */
+ibfs_status ibfs_server_wait(ibfs_server *s, uint64_t qid, int32_t timeout_ms,
+                             void *depth_out, uint32_t flags, ibfs_query_info *info);
+ibfs_status ibfs_server_stats_get(ibfs_server *s, ibfs_server_stats *out);
+ibfs_status ibfs_server_destroy(ibfs_server *s);
+
+/* Per-graph tuning (no counterpart in the reference, whose constants are
+   fixed at comm.h:25-30 and ibfs.cu:71-72): coordinate descent over width,
+   alpha/beta, queue thresholds, CTA size and concurrent batches, each trial
+   a real persistent run of `src` (device output, `reps` timed repeats).
+   `best` receives the winner; `log` (optional) one JSON object per trial. */
+ibfs_status ibfs_autotune(ibfs_graph *g, const int32_t *src_host, int64_t n,
+                          const ibfs_opts *base, int32_t reps, ibfs_opts *best,
+                          double *best_gteps, char *log, int32_t log_cap);
+
 /* TEPS numerator on the host: sum over sources of deg(v) for reached v
    (validate.h:59-76) of a source-major depth array. */
 ibfs_status ibfs_teps(const ibfs_graph *g, const void *depth_host, int64_t n,
