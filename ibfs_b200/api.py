@@ -42,13 +42,15 @@ class Opts(C.Structure):
         ("lrg_shed", C.c_int32), ("mode", C.c_int32), ("groupby", C.c_int32),
         ("depth_bytes", C.c_int32), ("groups", C.c_int32), ("threads", C.c_int32),
         ("ctas_per_sm", C.c_int32), ("use_graph", C.c_int32), ("timeout_ms", C.c_int32),
-        ("max_levels", C.c_int32), ("debug_withhold", C.c_int32), ("reserved", C.c_int32 * 7),
+        ("max_levels", C.c_int32), ("debug_withhold", C.c_int32), ("occupancy", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 
 class LevelRec(C.Structure):
     _fields_ = [("batch", C.c_int32), ("level", C.c_int32), ("dir", C.c_int32), ("pad", C.c_int32),
-                ("frontier", C.c_int64), ("frontier_edges", C.c_int64)]
+                ("frontier", C.c_int64), ("frontier_edges", C.c_int64), ("expand_ns", C.c_int64),
+                ("inspect_ns", C.c_int64)]
 
 
 class Stats(C.Structure):
@@ -425,7 +427,8 @@ def _levels(recs, st: Stats) -> list:
     if recs is None:
         return []
     return [dict(batch=recs[i].batch, level=recs[i].level, dir=recs[i].dir,
-                 frontier=recs[i].frontier, frontier_edges=recs[i].frontier_edges)
+                 frontier=recs[i].frontier, frontier_edges=recs[i].frontier_edges,
+                 expand_ns=recs[i].expand_ns, inspect_ns=recs[i].inspect_ns)
             for i in range(st.levels_len)]
 
 

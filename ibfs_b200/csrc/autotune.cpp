@@ -67,9 +67,9 @@ extern "C" ibfs_status ibfs_autotune(ibfs_graph* g, const int32_t* src, int64_t 
   auto note = [&](const Trial& t) {
     char buf[256];
     std::snprintf(buf, sizeof(buf),
-                  "{\"width\":%d,\"concurrent\":%d,\"sml\":%d,\"lrg\":%d,\"threads\":%d,"
+                  "{\"width\":%d,\"concurrent\":%d,\"sml\":%d,\"lrg\":%d,\"occupancy\":%d,"
                   "\"alpha\":%g,\"beta\":%g,\"groups\":%d,\"ms\":%.4f,\"gteps\":%.2f}\n",
-                  t.o.width, t.o.concurrent, t.o.sml_shed, t.o.lrg_shed, t.o.threads, t.o.alpha,
+                  t.o.width, t.o.concurrent, t.o.sml_shed, t.o.lrg_shed, t.o.occupancy, t.o.alpha,
                   t.o.beta, t.o.groups, t.ms, t.gteps);
     text += buf;
   };
@@ -100,7 +100,7 @@ extern "C" ibfs_status ibfs_autotune(ibfs_graph* g, const int32_t* src, int64_t 
   const float alphas[] = {1.0f, 2.0f, 4.0f, 8.0f, 14.0f, 32.0f};
   const float betas[] = {8.0f, 24.0f, 64.0f, 256.0f};
   const int thr[][2] = {{16, 256}, {32, 512}, {64, 1024}, {32, 4096}, {8, 128}};
-  const int threads[] = {256, 512};
+  const int occ[] = {0, 1, 2};
   const int groups[] = {0, 1, 2, 4};
   s = try_set([&](ibfs_opts& o, int i) {
         o.width = widths[i];
@@ -118,7 +118,7 @@ extern "C" ibfs_status ibfs_autotune(ibfs_graph* g, const int32_t* src, int64_t 
           return true;
         }, 5);
   if (s == IBFS_OK)
-    s = try_set([&](ibfs_opts& o, int i) { o.threads = threads[i]; return true; }, 2);
+    s = try_set([&](ibfs_opts& o, int i) { o.occupancy = occ[i]; return true; }, 3);
   if (s == IBFS_OK)
     s = try_set([&](ibfs_opts& o, int i) { o.groups = groups[i]; return true; }, 4);
   cudaFree(dout);

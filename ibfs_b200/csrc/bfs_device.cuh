@@ -46,7 +46,8 @@ struct Par {
   unsigned long long teps;     // sum over new (v, s) pairs of deg(v)
   uint32_t fmask[kMaxWords];   // OR of all new bits (sources still expanding)
   int32_t range_err;           // a level did not fit the depth type
-  int32_t pad[3];
+  int32_t hq_cnt;              // deferred bottom-up hub chunks of this level
+  int32_t pad[2];
 };
 
 // Control block of one group (one batch at a time).  256-byte aligned.
@@ -72,6 +73,7 @@ struct BatchRec {
 struct LevelRec {
   int32_t batch, level, dir, pad;
   long long frontier, frontier_edges;
+  long long expand_ns, inspect_ns;  // device time of the level's phases (persistent)
 };
 
 struct GroupBufs {
@@ -82,6 +84,7 @@ struct GroupBufs {
   int32_t* qs;
   int32_t* qm;
   int2* ql;
+  int2* hq;          // deferred bottom-up hub chunks (v, chunk)
   Ctl* ctl;
 };
 
@@ -110,7 +113,12 @@ struct Params {
   int lrec_cap;
   int vec_out;  // vertex-major rows allow 4-byte stores (n_b*db % 4 == 0, aligned base)
   int vec_sm;   // source-major rows allow 4-vertex stores (V % 4 == 0, aligned base)
+  int hub_t;        // bottom-up: a warp scans at most hub_t neighbours of a vertex;
+                    // a hub still missing bits defers the rest in chunks
 };
+
+constexpr int kHubScan = 1024;   // neighbours one warp scans before deferring
+constexpr int kHubChunk = 2048;  // edges per deferred chunk (one CTA each)
 
 // A team is the set of threads that share one batch: the whole grid in the
 // plain schedule, the CTAs of one group in the persistent kernel.
@@ -314,9 +322,56 @@ __device__ __forceinline__ void zero_plane_if_first(const Params& p, const Group
 // Phase: inspect level L (reads the level-L bitmap, fixes last, updates the
 // depth bit-planes, counters).
 // ---------------------------------------------------------------------------
+// Per changed vertex v of level L: new bits, last = curr, counters, planes.
+template <int WORDS>
+__device__ __forceinline__ void inspect_vertex(const Params& p, const GroupBufs& gb, long long v,
+                                               int level, bool depth_ok,
+                                               const uint32_t (&full)[WORDS], uint32_t (&fm)[WORDS],
+                                               unsigned long long& mf, unsigned long long& cnt,
+                                               unsigned long long& cdeg,
+                                               unsigned long long& teps) {
+  uint32_t c[WORDS], l[WORDS], nb[WORDS];
+  ld_status<WORDS>(gb.curr + (size_t)v * WORDS, c);
+  ld_status<WORDS>(gb.last + (size_t)v * WORDS, l);
+  bool comp = true;
+  uint32_t pop = 0;
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) {
+    nb[k] = c[k] & ~l[k];
+    comp = comp && (c[k] == full[k]);
+    pop += __popc(nb[k]);
+    fm[k] |= nb[k];
+  }
+  st_status<WORDS>(gb.last + (size_t)v * WORDS, c);
+  const long long deg = p.beg[v + 1] - p.beg[v];
+  mf += deg;
+  cnt += 1;
+  teps += (unsigned long long)deg * pop;
+  if (comp) cdeg += deg;
+  if (depth_ok) {
+    // depth(v, s) = level for the new bits: OR them into the planes of the
+    // level's set bits (one coalesced read-modify-write per plane).
+    for (int b = 0; (level >> b) != 0; b++) {
+      if (!((level >> b) & 1)) continue;
+      uint32_t* q = gb.planes + (size_t)b * p.plane_stride + (size_t)v * WORDS;
+      uint32_t x[WORDS];
+      ld_status<WORDS>(q, x);
+#pragma unroll
+      for (int k = 0; k < WORDS; k++) x[k] |= nb[k];
+      st_status<WORDS>(q, x);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Phase: inspect level L (reads the level-L bitmap, fixes last, updates the
+// depth bit-planes, counters).  `dense` picks the walk: one bitmap word per
+// warp step spread over all warps (many changed vertices), or 128 words per
+// warp step with only the non-empty words visited (few changed vertices).
+// ---------------------------------------------------------------------------
 template <int WORDS>
 __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par, int n_b,
-                              int level, bool depth_ok, const Team& t) {
+                              int level, bool depth_ok, bool dense, const Team& t) {
   uint32_t full[WORDS];
 #pragma unroll
   for (int k = 0; k < WORDS; k++) full[k] = full_word(n_b, k);
@@ -325,41 +380,39 @@ __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par, in
 #pragma unroll
   for (int k = 0; k < WORDS; k++) fm[k] = 0;
   const uint32_t* chg = chg_at(gb, p, level);
+  // the bitmap of level+1 (last used by level-1's expand) must start empty:
+  // bottom-up merges into it with atomics
+  zero_words(chg_at(gb, p, level + 1), p.chg_stride, t);
   const int lane = t.lane;
-  for (long long w = t.warp; w < p.nchg; w += t.nwarps) {
-    const uint32_t bits = __ldcg(chg + w);
-    if (!bits) continue;
-    const long long v = w * 32 + lane;
-    if (!((bits >> lane) & 1u)) continue;
-    uint32_t c[WORDS], l[WORDS], nb[WORDS];
-    ld_status<WORDS>(gb.curr + (size_t)v * WORDS, c);
-    ld_status<WORDS>(gb.last + (size_t)v * WORDS, l);
-    bool comp = true;
-    uint32_t pop = 0;
-#pragma unroll
-    for (int k = 0; k < WORDS; k++) {
-      nb[k] = c[k] & ~l[k];
-      comp = comp && (c[k] == full[k]);
-      pop += __popc(nb[k]);
-      fm[k] |= nb[k];
+  if (dense) {
+    for (long long w = t.warp; w < p.nchg; w += t.nwarps) {
+      const uint32_t bits = __ldcg(chg + w);
+      if (!bits) continue;
+      const long long v = w * 32 + lane;
+      if ((bits >> lane) & 1u)
+        inspect_vertex<WORDS>(p, gb, v, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
     }
-    st_status<WORDS>(gb.last + (size_t)v * WORDS, c);
-    const long long deg = p.beg[v + 1] - p.beg[v];
-    mf += deg;
-    cnt += 1;
-    teps += (unsigned long long)deg * pop;
-    if (comp) cdeg += deg;
-    if (depth_ok) {
-      // depth(v, s) = level for the new bits: OR them into the planes of
-      // the level's set bits (one coalesced read-modify-write per plane).
-      for (int b = 0; (level >> b) != 0; b++) {
-        if (!((level >> b) & 1)) continue;
-        uint32_t* q = gb.planes + (size_t)b * p.plane_stride + (size_t)v * WORDS;
-        uint32_t x[WORDS];
-        ld_status<WORDS>(q, x);
-#pragma unroll
-        for (int k = 0; k < WORDS; k++) x[k] |= nb[k];
-        st_status<WORDS>(q, x);
+  } else {
+    const long long nblk = (p.nchg + 127) / 128;
+    for (long long blk = t.warp; blk < nblk; blk += t.nwarps) {
+      const uint4 q4 = __ldcg(reinterpret_cast<const uint4*>(chg) + blk * 32 + lane);
+      uint32_t nzl = __ballot_sync(0xFFFFFFFFu, (q4.x | q4.y | q4.z | q4.w) != 0u);
+      while (nzl) {
+        const int src = __ffs(nzl) - 1;
+        nzl &= nzl - 1;
+        const uint32_t b0 = __shfl_sync(0xFFFFFFFFu, q4.x, src);
+        const uint32_t b1 = __shfl_sync(0xFFFFFFFFu, q4.y, src);
+        const uint32_t b2 = __shfl_sync(0xFFFFFFFFu, q4.z, src);
+        const uint32_t b3 = __shfl_sync(0xFFFFFFFFu, q4.w, src);
+        const long long w0 = blk * 128 + src * 4;
+        if ((b0 >> lane) & 1u)
+          inspect_vertex<WORDS>(p, gb, (w0 + 0) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
+        if ((b1 >> lane) & 1u)
+          inspect_vertex<WORDS>(p, gb, (w0 + 1) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
+        if ((b2 >> lane) & 1u)
+          inspect_vertex<WORDS>(p, gb, (w0 + 2) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
+        if ((b3 >> lane) & 1u)
+          inspect_vertex<WORDS>(p, gb, (w0 + 3) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
       }
     }
   }
@@ -370,6 +423,12 @@ __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par, in
   cta_add_u64(&par->teps, teps);
 #pragma unroll
   for (int k = 0; k < WORDS; k++) cta_or_u32(&par->fmask[k], fm[k]);
+}
+
+// Whether the inspect of the next level should use the dense walk: its
+// changed set is at most the previous frontier's neighbourhood.
+__host__ __device__ inline bool inspect_dense(unsigned long long prev_mf, long long V) {
+  return prev_mf * 16ull > (unsigned long long)V;
 }
 
 // ---------------------------------------------------------------------------
@@ -385,10 +444,22 @@ __device__ inline void qbuild_phase(const Params& p, const GroupBufs& gb, int le
   const uint32_t lt = (1u << lane) - 1u;
   const uint32_t* prev = chg_at(gb, p, level - 1);
   uint32_t* next = chg_at(gb, p, level);
-  for (long long w = t.warp; w < p.nchg; w += t.nwarps) {
-    const uint32_t bits = __ldcg(prev + w);
-    if (lane == 0) __stcg(next + w, 0u);
+  const long long nblk = (p.nchg + 127) / 128;
+  for (long long blk = t.warp; blk < nblk; blk += t.nwarps) {
+   const uint4 q4 = __ldcg(reinterpret_cast<const uint4*>(prev) + blk * 32 + lane);
+   __stcg(reinterpret_cast<uint4*>(next) + blk * 32 + lane, make_uint4(0, 0, 0, 0));
+   uint32_t nzl = __ballot_sync(0xFFFFFFFFu, (q4.x | q4.y | q4.z | q4.w) != 0u);
+   while (nzl) {
+    const int src_lane = __ffs(nzl) - 1;
+    nzl &= nzl - 1;
+    const uint32_t qw[4] = {__shfl_sync(0xFFFFFFFFu, q4.x, src_lane),
+                            __shfl_sync(0xFFFFFFFFu, q4.y, src_lane),
+                            __shfl_sync(0xFFFFFFFFu, q4.z, src_lane),
+                            __shfl_sync(0xFFFFFFFFu, q4.w, src_lane)};
+    for (int kk = 0; kk < 4; kk++) {
+    const uint32_t bits = qw[kk];
     if (!bits) continue;
+    const long long w = blk * 128 + src_lane * 4 + kk;
     const long long v = w * 32 + lane;
     const bool mine = (bits >> lane) & 1u;
     long long deg = 0;
@@ -425,6 +496,8 @@ __device__ inline void qbuild_phase(const Params& p, const GroupBufs& gb, int le
       const int first = base + incl - nch;
       for (int c = 0; c < nch; c++) gb.ql[first + c] = make_int2((int)v, c);
     }
+    }
+   }
   }
 }
 
@@ -501,6 +574,92 @@ __device__ void td_phase(const Params& p, const GroupBufs& gb, int level, const 
   }
 }
 
+// Second bottom-up stage: the hubs that were still missing frontier bits
+// after their first hub_t neighbours.  One CTA per chunk of kHubChunk edges
+// (frontier neighbours only); a chunk is skipped when curr[v], which the
+// other chunks of the same hub merge into with atomics, already covers
+// every frontier bit.  So one hub's long scan is spread over many CTAs
+// instead of holding one warp -- and the whole level -- for its adjacency.
+template <int WORDS>
+__device__ void bu_defer_phase(const Params& p, const GroupBufs& gb, int level,
+                               const uint32_t* fmask_g, const int32_t* hq_cnt, const Team& t) {
+  __shared__ uint32_t s_acc[32][kMaxWords];
+  __shared__ uint32_t s_cur[kMaxWords];
+  __shared__ int s_skip;
+  uint32_t fm[WORDS];
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) fm[k] = __ldcg(fmask_g + k);
+  const uint32_t* front = chg_at(gb, p, level - 1);
+  uint32_t* out = chg_at(gb, p, level);
+  const int n = __ldcg(hq_cnt);
+  const int lane = t.lane, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c = t.block; c < n; c += t.nblocks) {
+    const int2 hc = gb.hq[c];
+    const int32_t v = hc.x;
+    if (threadIdx.x == 0) {  // one read, so that the skip decision is uniform
+      uint32_t cur[WORDS];
+      ld_status<WORDS>(gb.curr + (size_t)v * WORDS, cur);
+      bool need = false;
+#pragma unroll
+      for (int k = 0; k < WORDS; k++) {
+        s_cur[k] = cur[k];
+        need |= (fm[k] & ~cur[k]) != 0u;
+      }
+      s_skip = need ? 0 : 1;
+    }
+    __syncthreads();
+    if (s_skip) {
+      __syncthreads();
+      continue;
+    }
+    const long long e_end = p.beg[v + 1];
+    const long long b0 = p.beg[v] + p.hub_t + (long long)hc.y * kHubChunk;
+    const long long b1 = min(e_end, b0 + (long long)kHubChunk);
+    uint32_t acc[WORDS];
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) acc[k] = 0;
+    for (long long e = b0 + threadIdx.x; e < b1; e += blockDim.x) {
+      const int32_t u = p.col[e];
+      if (!((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u)) continue;
+      uint32_t x[WORDS];
+      ld_status<WORDS>(gb.last + (size_t)u * WORDS, x);
+#pragma unroll
+      for (int k = 0; k < WORDS; k++) acc[k] |= x[k];
+    }
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) {
+      const uint32_t r = __reduce_or_sync(0xFFFFFFFFu, acc[k]);
+      if (lane == 0) s_acc[wid][k] = r;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t nb[WORDS];
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k < WORDS; k++) {
+        uint32_t r = 0;
+        for (int i = 0; i < nw; i++) r |= s_acc[i][k];
+        nb[k] = r & ~s_cur[k];
+        any |= nb[k] != 0u;
+      }
+      if (any) {
+        if constexpr (WORDS == 1) {
+          atomicOr(gb.curr + v, nb[0]);
+        } else {
+          unsigned long long* q = reinterpret_cast<unsigned long long*>(gb.curr + (size_t)v * WORDS);
+#pragma unroll
+          for (int k = 0; k < WORDS / 2; k++) {
+            const unsigned long long w2 = ((unsigned long long)nb[2 * k + 1] << 32) | nb[2 * k];
+            if (w2) atomicOr(q + k, w2);
+          }
+        }
+        atomicOr(out + (v >> 5), 1u << (v & 31));
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Phase: bottom-up level L.  Every vertex that still lacks a bit of the
 // previous level's frontier mask ORs the `last` words of those neighbours
@@ -515,7 +674,7 @@ __device__ void td_phase(const Params& p, const GroupBufs& gb, int level, const 
 // ---------------------------------------------------------------------------
 template <int WORDS>
 __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
-                         const uint32_t* fmask_g, const Team& t) {
+                         const uint32_t* fmask_g, int32_t* hq_cnt, const Team& t) {
   uint32_t fm[WORDS];
 #pragma unroll
   for (int k = 0; k < WORDS; k++) fm[k] = __ldcg(fmask_g + k);
@@ -581,22 +740,31 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
       uint32_t a[WORDS];
 #pragma unroll
       for (int k = 0; k < WORDS; k++) a[k] = __shfl_sync(0xFFFFFFFFu, acc[k], j);
-      for (long long e = e0; e < e1; e += 32) {
+      // a warp scans at most hub_t neighbours; the rest of a hub that is
+      // still missing frontier bits is deferred to bu_defer_phase
+      const long long e_lim = (e1 - e0 > p.hub_t) ? e0 + p.hub_t : e1;
+      bool miss = true;
+      for (long long e = e0; e < e_lim; e += 32) {
         uint32_t x[WORDS];
 #pragma unroll
         for (int k = 0; k < WORDS; k++) x[k] = 0;
-        if (e + lane < e1) {
+        if (e + lane < e_lim) {
           const int32_t u = p.col[e + lane];
           if ((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u)
             ld_status<WORDS>(gb.last + (size_t)u * WORDS, x);
         }
-        bool miss = false;
+        miss = false;
 #pragma unroll
         for (int k = 0; k < WORDS; k++) {
           a[k] |= __reduce_or_sync(0xFFFFFFFFu, x[k]);
           miss |= (fm[k] & ~a[k]) != 0u;
         }
         if (!miss) break;
+      }
+      if (miss && e_lim < e1 && lane == 0) {
+        const int nch = (int)((e1 - e_lim + kHubChunk - 1) / kHubChunk);
+        const int base0 = atomicAdd(hq_cnt, nch);
+        for (int c = 0; c < nch; c++) gb.hq[base0 + c] = make_int2((int)(base + j), c);
       }
       if (lane == j) {
 #pragma unroll
@@ -609,7 +777,7 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
     ch = ch && need;
     if (ch) st_status<WORDS>(gb.curr + (size_t)v * WORDS, acc);
     const uint32_t bal = __ballot_sync(0xFFFFFFFFu, ch);
-    if (lane == 0) __stcg(out + (base >> 5), bal);
+    if (lane == 0 && bal) atomicOr(out + (base >> 5), bal);
   }
 }
 

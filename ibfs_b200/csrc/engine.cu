@@ -55,9 +55,11 @@ __device__ __forceinline__ void load_rows(const Params& p, int b, int n_b, int32
   __syncthreads();
 }
 
-template <int WORDS>
-__global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
-  __shared__ int s_dir, s_stop, s_err, s_maxl;
+// THREADS x MINB fixes the register budget (65536 / (THREADS * MINB)) and
+// hence how many warps per SM hide the latency of the random gathers.
+template <int WORDS, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) persistent_kernel(Params p) {
+  __shared__ int s_dir, s_stop, s_err, s_maxl, s_dense;
   __shared__ int32_t s_rows[kMaxWords * 32];
   const int g = blockIdx.x / p.cpg;
   const Team t = make_team(blockIdx.x % p.cpg, p.cpg);
@@ -88,10 +90,11 @@ __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
     BARRIER();
     seed_phase<WORDS>(p, gb, p.src + k0, n_b, t);
     BARRIER();
-    inspect_phase<WORDS>(p, gb, &ctl->par[0], n_b, 0, true, t);
+    inspect_phase<WORDS>(p, gb, &ctl->par[0], n_b, 0, true, false, t);
     BARRIER();
     int level = 0, cur_dir = kDirTD, max_level = 0, td = 0, bu = 0;
     unsigned long long m_u = (unsigned long long)p.E, teps = 0;
+    unsigned long long t_lvl = global_ns(), t_mid = t_lvl;
     int err = 0;
     while (true) {
       if (threadIdx.x == 0) {
@@ -111,6 +114,10 @@ __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
             LevelRec r;
             r.batch = b; r.level = level; r.dir = level == 0 ? -1 : cur_dir; r.pad = 0;
             r.frontier = (long long)changed; r.frontier_edges = (long long)mf;
+            const unsigned long long t_now = global_ns();
+            r.expand_ns = (long long)(t_mid - t_lvl);
+            r.inspect_ns = (long long)(t_now - t_mid);
+            t_lvl = t_now;
             p.lrec[(size_t)b * p.lrec_cap + level] = r;
           }
           if (!stop) {
@@ -122,14 +129,17 @@ __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
         s_stop = stop;
         s_err = err;
         s_maxl = max_level;
+        s_dense = inspect_dense(mf, p.V) ? 1 : 0;
       }
       __syncthreads();
       const int stop = s_stop;
+      const bool dense = s_dense != 0;
       cur_dir = s_dir;
       err = s_err;
       __syncthreads();
       if (stop) break;
       level++;
+      bool continue_inspect = false;
       zero_plane_if_first(p, gb, level, t);
       if (cur_dir == kDirTD) {
         td++;
@@ -138,11 +148,23 @@ __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
         td_phase<WORDS>(p, gb, level, ctl->qc[level & 1], t);
       } else {
         bu++;
-        bu_phase<WORDS>(p, gb, level, ctl->par[(level - 1) & 1].fmask, t);
+        bu_phase<WORDS>(p, gb, level, ctl->par[(level - 1) & 1].fmask,
+                        &ctl->par[level & 1].hq_cnt, t);
+        BARRIER();
+        if (__ldcg(&ctl->par[level & 1].hq_cnt) > 0) {  // same value in every CTA
+          bu_defer_phase<WORDS>(p, gb, level, ctl->par[(level - 1) & 1].fmask,
+                                &ctl->par[level & 1].hq_cnt, t);
+          BARRIER();
+        }
+        if (lead) t_mid = global_ns();
+        continue_inspect = true;
       }
-      BARRIER();
+      if (!continue_inspect) {
+        BARRIER();
+        if (lead) t_mid = global_ns();
+      }
       inspect_phase<WORDS>(p, gb, &ctl->par[level & 1], n_b, level,
-                           level <= depth_limit(p.db), t);
+                           level <= depth_limit(p.db), dense, t);
       BARRIER();
     }
     if (err) {
@@ -153,6 +175,15 @@ __global__ void __launch_bounds__(512, 2) persistent_kernel(Params p) {
       return;
     }
     output_phase<WORDS>(p, gb, batch_depth(p, b), s_rows, n_b, s_maxl, t);
+    if (lead && level + 1 < p.lrec_cap) {
+      // one extra record per batch: dir 2 = the output pass
+      LevelRec r;
+      r.batch = b; r.level = level + 1; r.dir = 2; r.pad = 0;
+      r.frontier = 0; r.frontier_edges = 0;
+      r.expand_ns = (long long)(global_ns() - t_lvl);
+      r.inspect_ns = 0;
+      p.lrec[(size_t)b * p.lrec_cap + level + 1] = r;
+    }
     if (lead) {
       BatchRec r;
       r.levels = level;
@@ -179,11 +210,13 @@ __global__ void __launch_bounds__(512) k_seed(Params p, int b) {
 }
 
 template <int WORDS>
-__global__ void __launch_bounds__(512) k_inspect(Params p, GroupBufs gb, int b, int level) {
+__global__ void __launch_bounds__(512) k_inspect(Params p, GroupBufs gb, int b, int level,
+                                                 int dense) {
   const Team t = make_team(blockIdx.x, gridDim.x);
   const long long k0 = (long long)b * p.C;
   const int n_b = (int)min((long long)p.C, p.n_total - k0);
-  inspect_phase<WORDS>(p, gb, &gb.ctl->par[level & 1], n_b, level, level <= depth_limit(p.db), t);
+  inspect_phase<WORDS>(p, gb, &gb.ctl->par[level & 1], n_b, level, level <= depth_limit(p.db),
+                       dense != 0, t);
 }
 
 __global__ void __launch_bounds__(512) k_qbuild(Params p, GroupBufs gb, int level) {
@@ -200,7 +233,15 @@ __global__ void __launch_bounds__(512) k_td(Params p, GroupBufs gb, int level) {
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_bu(Params p, GroupBufs gb, int level) {
   const Team t = make_team(blockIdx.x, gridDim.x);
-  bu_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask, t);
+  bu_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
+                  &gb.ctl->par[level & 1].hq_cnt, t);
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_bu_defer(Params p, GroupBufs gb, int level) {
+  const Team t = make_team(blockIdx.x, gridDim.x);
+  bu_defer_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
+                        &gb.ctl->par[level & 1].hq_cnt, t);
 }
 
 template <int WORDS>
@@ -280,10 +321,10 @@ struct PinBuf {
 };
 
 struct GroupMem {
-  DevBuf last, curr, chg, qs, qm, ql, ctl, planes;
+  DevBuf last, curr, chg, qs, qm, ql, hq, ctl, planes;
   void release() {
     last.release(); curr.release(); chg.release(); qs.release();
-    qm.release(); ql.release(); ctl.release(); planes.release();
+    qm.release(); ql.release(); hq.release(); ctl.release(); planes.release();
   }
 };
 
@@ -307,6 +348,7 @@ struct ibfs_graph {
   int64_t V = 0, E = 0, max_deg = 0;
   HostCsr h;
   DevBuf beg, col;
+  int64_t defer_cap = 16;  // bound on deferred bottom-up hub chunks per level
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -343,22 +385,34 @@ static ibfs_status check_opts(const ibfs_opts* o) {
 static size_t group_bytes(int64_t V, int64_t E, int words, int C, int db, int lrg, int chunk,
                           bool /*unused*/) {
   const size_t vpad = (size_t)((V + 31) & ~31LL);
-  const size_t nchg = (size_t)(((V + 31) / 32 + 3) & ~3LL);
+  const size_t nchg = (size_t)(((V + 31) / 32 + 127) & ~127LL);
   const size_t capl = (size_t)(E / std::max(chunk, 1) + std::min<int64_t>(V, E / std::max(lrg, 1)) + 16);
   size_t b = 2 * vpad * words * 4 + nchg * 4 + 2 * (size_t)V * 4 + capl * 8 + sizeof(Ctl);
   b += (size_t)(db == 1 ? 8 : 16) * vpad * words * 4 + nchg * 4;  // planes + 2nd bitmap
   return b;
 }
 
-template <int WORDS>
-static const void* persistent_fn() { return (const void*)persistent_kernel<WORDS>; }
+// Occupancy levels of the persistent kernel: (threads per CTA, CTAs per SM
+// the register budget is sized for).
+static const int kOccThreads[4] = {512, 256, 256, 512};
+static const int kOccMinB[4] = {2, 6, 8, 1};
 
-static const void* persistent_for(int words) {
+template <int WORDS>
+static const void* persistent_fn(int level) {
+  switch (level) {
+    case 1: return (const void*)persistent_kernel<WORDS, 256, 6>;
+    case 2: return (const void*)persistent_kernel<WORDS, 256, 8>;
+    case 3: return (const void*)persistent_kernel<WORDS, 512, 1>;
+    default: return (const void*)persistent_kernel<WORDS, 512, 2>;
+  }
+}
+
+static const void* persistent_for(int words, int level = 0) {
   switch (words) {
-    case 1: return persistent_fn<1>();
-    case 2: return persistent_fn<2>();
-    case 4: return persistent_fn<4>();
-    default: return persistent_fn<8>();
+    case 1: return persistent_fn<1>(level);
+    case 2: return persistent_fn<2>(level);
+    case 4: return persistent_fn<4>(level);
+    default: return persistent_fn<8>(level);
   }
 }
 
@@ -370,14 +424,15 @@ static cudaError_t launch_plain_level(const Params& p, const GroupBufs& gb, int 
     k_td<WORDS><<<grid, threads, 0, s>>>(p, gb, level);
   } else {
     k_bu<WORDS><<<grid, threads, 0, s>>>(p, gb, level);
+    k_bu_defer<WORDS><<<grid, threads, 0, s>>>(p, gb, level);
   }
   return cudaGetLastError();
 }
 
 template <int WORDS>
 static cudaError_t launch_plain_inspect(const Params& p, const GroupBufs& gb, int grid, int threads,
-                                        int b, int level, cudaStream_t s) {
-  k_inspect<WORDS><<<grid, threads, 0, s>>>(p, gb, b, level);
+                                        int b, int level, int dense, cudaStream_t s) {
+  k_inspect<WORDS><<<grid, threads, 0, s>>>(p, gb, b, level, dense);
   return cudaGetLastError();
 }
 
@@ -411,7 +466,7 @@ static ibfs_status ensure_workspace(ibfs_graph* g, const RunPlan& rp, const ibfs
                                     int layout) {
   (void)layout;
   const size_t vpad = (size_t)((g->V + 31) & ~31LL);
-  const size_t nchg = (size_t)(((g->V + 31) / 32 + 3) & ~3LL);
+  const size_t nchg = (size_t)(((g->V + 31) / 32 + 127) & ~127LL);
   const int chunk = rp.threads * 4;
   const size_t capl = (size_t)(g->E / chunk + std::min<int64_t>(g->V, g->E / std::max(o.lrg_shed, 1)) + 16);
   if ((int)g->groups.size() < rp.G) g->groups.resize(rp.G);
@@ -426,6 +481,7 @@ static ibfs_status ensure_workspace(ibfs_graph* g, const RunPlan& rp, const ibfs
     if ((s = m.qs.ensure((size_t)g->V * 4)) != IBFS_OK) return s;
     if ((s = m.qm.ensure((size_t)g->V * 4)) != IBFS_OK) return s;
     if ((s = m.ql.ensure(capl * 8)) != IBFS_OK) return s;
+    if ((s = m.hq.ensure((size_t)g->defer_cap * 8)) != IBFS_OK) return s;
     if ((s = m.ctl.ensure(sizeof(Ctl))) != IBFS_OK) return s;
   }
   return IBFS_OK;
@@ -475,7 +531,7 @@ extern "C" void ibfs_opts_default(ibfs_opts* o) {
   o->width = 128;
   o->concurrent = 0;
   o->switch_level = -1;
-  o->alpha = 14.0f;
+  o->alpha = 4.0f;
   o->beta = 24.0f;
   o->sml_shed = 32;
   o->lrg_shed = 512;
@@ -544,6 +600,15 @@ static ibfs_status upload_graph(ibfs_graph* g) {
   int64_t md = 0;
   for (int64_t v = 0; v < g->V; v++) md = std::max(md, g->h.beg[v + 1] - g->h.beg[v]);
   g->max_deg = md;
+  // bound on the bottom-up hub chunks one level can defer
+  {
+    int64_t cap = 16;
+    for (int64_t v = 0; v < g->V; v++) {
+      const int64_t d = g->h.beg[v + 1] - g->h.beg[v];
+      if (d > kHubScan) cap += (d - kHubScan + kHubChunk - 1) / kHubChunk;
+    }
+    g->defer_cap = cap;
+  }
   return IBFS_OK;
 }
 
@@ -753,14 +818,16 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   rp.words = words_for(o.width);
   rp.C = o.concurrent ? o.concurrent : o.width;
   rp.nbatches = (int)((n + rp.C - 1) / rp.C);
-  rp.threads = o.threads ? o.threads : 512;
+  const int occ_level = (o.occupancy >= 0 && o.occupancy <= 3) ? o.occupancy : 0;
+  rp.threads = o.mode == IBFS_MODE_PERSISTENT ? kOccThreads[occ_level]
+                                              : (o.threads ? o.threads : 512);
   rp.db = db;
   rp.host_out = !(flags & IBFS_OUT_DEVICE);
   rp.smem = 0;
   const bool persistent = o.mode == IBFS_MODE_PERSISTENT;
   // grid sizing
   int occ = 0;
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, persistent_for(rp.words), rp.threads,
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, persistent_for(rp.words, occ_level), rp.threads,
                                                    rp.smem));
   if (occ < 1) return IBFS_ERR_UNSUPPORTED;
   int per_sm = o.ctas_per_sm ? std::min(o.ctas_per_sm, occ) : occ;
@@ -836,6 +903,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     hgb[i].qs = m.qs.as<int32_t>();
     hgb[i].qm = m.qm.as<int32_t>();
     hgb[i].ql = m.ql.as<int2>();
+    hgb[i].hq = m.hq.as<int2>();
     hgb[i].ctl = m.ctl.as<Ctl>();
     hgb[i].planes = m.planes.as<uint32_t>();
   }
@@ -846,7 +914,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   p.V = g->V;
   p.E = g->E;
   p.nchg = (g->V + 31) / 32;
-  p.chg_stride = (p.nchg + 3) & ~3LL;
+  p.chg_stride = (p.nchg + 127) & ~127LL;  // whole 128-word blocks (vector bitmap walks)
   p.plane_stride = (long long)((g->V + 31) & ~31LL) * rp.words;
   p.src = g->d_src.as<int32_t>();
   p.out_row = g->d_outrow.as<int32_t>();
@@ -873,6 +941,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   p.lrec = g->d_lrec.as<LevelRec>();
   p.lrec_cap = kLrecCap;
   p.vec_out = (rp.C % 4 == 0) && ((reinterpret_cast<uintptr_t>(dout) & 3) == 0);
+  p.hub_t = kHubScan;
   p.vec_sm = (g->V % 4 == 0) && ((reinterpret_cast<uintptr_t>(dout) & 3) == 0);
 
   int64_t launches = 0;
@@ -907,7 +976,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
       cfg.attrs = attr;
       cfg.numAttrs = 1;
       void* args[] = {&p};
-      CU(cudaLaunchKernelExC(&cfg, persistent_for(rp.words), args));
+      CU(cudaLaunchKernelExC(&cfg, persistent_for(rp.words, occ_level), args));
       launches += 1;
     }
     if (capturing) CU(cudaEventRecordWithFlags(g->ev1, cs, cudaEventRecordExternal));
@@ -965,14 +1034,14 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     BatchRec* hbr = g->h_brec.as<BatchRec>();
     LevelRec* hlr = g->h_lrec.as<LevelRec>();
     const size_t vpad = (size_t)((g->V + 31) & ~31LL);
-    const size_t nchg = (size_t)(((g->V + 31) / 32 + 3) & ~3LL);
+    const size_t nchg = (size_t)(((g->V + 31) / 32 + 127) & ~127LL);
     for (int b = 0; b < rp.nbatches; b++) {
       CU(cudaMemsetAsync(gb.last, 0, vpad * rp.words * 4, s));
       CU(cudaMemsetAsync(gb.curr, 0, vpad * rp.words * 4, s));
       CU(cudaMemsetAsync(gb.chg, 0, 2 * nchg * 4, s));
       CU(cudaMemsetAsync(gb.ctl, 0, sizeof(Ctl), s));
       CU(DISPATCH_WORDS(rp.words, launch_plain_seed, p, grid, thr, b, s));
-      CU(DISPATCH_WORDS(rp.words, launch_plain_inspect, p, gb, grid, thr, b, 0, s));
+      CU(DISPATCH_WORDS(rp.words, launch_plain_inspect, p, gb, grid, thr, b, 0, 0, s));
       launches += 2;
       int level = 0, cur_dir = kDirTD, max_level = 0, td = 0, bu = 0, err = 0;
       unsigned long long m_u = (unsigned long long)g->E, teps = 0;
@@ -993,6 +1062,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
           LevelRec& r = hlr[(size_t)b * kLrecCap + level];
           r.batch = b; r.level = level; r.dir = level == 0 ? -1 : cur_dir; r.pad = 0;
           r.frontier = (long long)pr.changed; r.frontier_edges = (long long)pr.mf;
+          r.expand_ns = r.inspect_ns = 0;
         }
         if (stop) break;
         cur_dir = nd;
@@ -1005,9 +1075,10 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
         CU(cudaMemsetAsync(&gb.ctl->par[level & 1], 0, sizeof(Par), s));
         CU(cudaMemsetAsync(&gb.ctl->qc[level & 1][0], 0, sizeof(int32_t) * 4, s));
         CU(DISPATCH_WORDS(rp.words, launch_plain_level, p, gb, grid, thr, level, cur_dir, s));
-        launches += cur_dir == kDirTD ? 2 : 1;
+        launches += 2;
         if (cur_dir == kDirTD) td++; else bu++;
-        CU(DISPATCH_WORDS(rp.words, launch_plain_inspect, p, gb, grid, thr, b, level, s));
+        CU(DISPATCH_WORDS(rp.words, launch_plain_inspect, p, gb, grid, thr, b, level,
+                          inspect_dense(pr.mf, p.V) ? 1 : 0, s));
         launches += 1;
       }
       BatchRec& r = hbr[b];
@@ -1068,11 +1139,13 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
       const LevelRec* lr = g->h_lrec.as<LevelRec>();
       int k = 0;
       for (int b = 0; b < rp.nbatches && k < st->levels_cap; b++)
-        for (int l = 0; l <= std::min(br[b].levels, kLrecCap - 1) && k < st->levels_cap; l++) {
+        for (int l = 0; l <= std::min(br[b].levels + (persistent ? 1 : 0), kLrecCap - 1) &&
+                        k < st->levels_cap; l++) {
           const LevelRec& r = lr[(size_t)b * kLrecCap + l];
           ibfs_level_rec& o2 = st->levels[k++];
           o2.batch = r.batch; o2.level = r.level; o2.dir = r.dir; o2.pad = 0;
           o2.frontier = r.frontier; o2.frontier_edges = r.frontier_edges;
+          o2.expand_ns = r.expand_ns; o2.inspect_ns = r.inspect_ns;
         }
       st->levels_len = k;
     }

@@ -88,7 +88,7 @@ extern "C" ibfs_status ibfs_run_static_scratch(const int64_t* beg_dev, const int
   const int chunk = threads * 4;
   const int lrg = 512;
   const size_t vpad = (size_t)((V + 31) & ~31LL);
-  const size_t nchg = (size_t)(((V + 31) / 32 + 3) & ~3LL);
+  const size_t nchg = (size_t)(((V + 31) / 32 + 127) & ~127LL);
   const size_t capl = (size_t)(E / chunk + (V < E / lrg ? V : E / lrg) + 16);
   size_t off = 0;
   const size_t o_gb = off; off = align256(off + sizeof(GroupBufs));
@@ -126,6 +126,7 @@ extern "C" ibfs_status ibfs_run_static_scratch(const int64_t* beg_dev, const int
   gb.qs = reinterpret_cast<int32_t*>(base + o_qs);
   gb.qm = reinterpret_cast<int32_t*>(base + o_qm);
   gb.ql = reinterpret_cast<int2*>(base + o_ql);
+  gb.hq = nullptr;
   gb.ctl = reinterpret_cast<Ctl*>(base + o_ctl);
   // What must start at zero: the control block (barrier, error, counters)
   // and the batch records.  Status words and bitmap are cleared per batch by
@@ -173,6 +174,7 @@ extern "C" ibfs_status ibfs_run_static_scratch(const int64_t* beg_dev, const int
   p.lrec = reinterpret_cast<LevelRec*>(base + o_lrec);
   p.lrec_cap = kLrecCap;
   p.vec_out = ((reinterpret_cast<uintptr_t>(depth_dev) & 3) == 0) ? 1 : 0;
+  p.hub_t = INT32_MAX;  // no deferred hub chunks here: the sweep scans whole lists
   p.vec_sm = 0;
   NA_CU(launch_persistent_params(p, words, p.cpg, threads, 0, s));
 

@@ -76,8 +76,8 @@ typedef struct ibfs_opts {
     int32_t switch_level;  /* >= 0: fixed switch as the reference's CLI argument:
                               top-down while level <= switch_level, bottom-up after;
                               -1: alpha/beta switching                            */
-    float alpha;           /* TD->BU when frontier_edges > unexplored_edges/alpha */
-    float beta;            /* BU->TD when frontier_vertices < V/beta              */
+    float alpha;           /* TD->BU when frontier_edges > unexplored_edges/alpha (4) */
+    float beta;            /* BU->TD when frontier_vertices < V/beta (24)         */
     int32_t sml_shed;      /* degree < sml_shed: one thread per vertex (default 32) */
     int32_t lrg_shed;      /* degree > lrg_shed: CTA chunks (default 512)         */
     int32_t mode;          /* ibfs_mode                                           */
@@ -92,7 +92,10 @@ typedef struct ibfs_opts {
     int32_t max_levels;    /* abort with IBFS_ERR_RANGE beyond this (0: 65534)    */
     int32_t debug_withhold;/* test hook: CTA 0 never arrives at its first grid
                               barrier, so every wait runs out (IBFS_ERR_TIMEOUT)  */
-    int32_t reserved[7];
+    int32_t occupancy;     /* persistent kernel register budget / warps per SM:
+                              0: 512 threads x 2 CTAs (64 regs), 1: 256 x 6 (42),
+                              2: 256 x 8 (32), 3: 512 x 1 (128)                 */
+    int32_t reserved[6];
 } ibfs_opts;
 
 typedef struct ibfs_level_rec {
@@ -102,6 +105,9 @@ typedef struct ibfs_level_rec {
     int32_t pad;
     int64_t frontier;      /* vertices whose status changed at this level         */
     int64_t frontier_edges;/* sum of their degrees                                */
+    int64_t expand_ns;     /* device time of the level's expand phase (persistent
+                              schedule; 0 otherwise; level 0: seeding)            */
+    int64_t inspect_ns;    /* device time of its inspect phase                    */
 } ibfs_level_rec;
 
 typedef struct ibfs_stats {

@@ -41,6 +41,7 @@ def test_opts_default_matches_reference_constants():
     assert o.width == 128  # comp_t = uint4 (comm.h:44)
     assert o.sml_shed == 32 and o.lrg_shed == 512  # ibfs.cu:71-72
     assert o.switch_level == -1
+    assert o.alpha == 4.0 and o.beta == 24.0
 
 
 def test_rmat_deterministic_and_clean():
