@@ -113,6 +113,8 @@ struct Params {
   int lrec_cap;
   int vec_out;  // vertex-major rows allow 4-byte stores (n_b*db % 4 == 0, aligned base)
   int vec_sm;   // source-major rows allow 4-vertex stores (V % 4 == 0, aligned base)
+  int bu_filter;    // bottom-up skips neighbours outside the previous frontier
+  int col_vec;      // col is 16-byte aligned and padded by 4 entries (vector reads)
   int hub_t;        // bottom-up: a warp scans at most hub_t neighbours of a vertex;
                     // a hub still missing bits defers the rest in chunks
 };
@@ -620,7 +622,7 @@ __device__ void bu_defer_phase(const Params& p, const GroupBufs& gb, int level,
     for (int k = 0; k < WORDS; k++) acc[k] = 0;
     for (long long e = b0 + threadIdx.x; e < b1; e += blockDim.x) {
       const int32_t u = p.col[e];
-      if (!((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u)) continue;
+      if (p.bu_filter && !((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u)) continue;
       uint32_t x[WORDS];
       ld_status<WORDS>(gb.last + (size_t)u * WORDS, x);
 #pragma unroll
@@ -703,15 +705,25 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
     need = need && valid && (b1 > b0);
     const bool small = need && (b1 - b0) <= p.but;
     if (small) {
-      // four neighbours in flight per step: the scan is latency bound
-      for (long long e = b0; e < b1; e += 4) {
+      // four neighbours in flight per step; with col_vec their ids are one
+      // aligned 16-byte vector (col is padded by 4 entries at its end)
+      const int4* col4 = reinterpret_cast<const int4*>(p.col);
+      const long long a0 = p.col_vec ? (b0 & ~3LL) : b0;
+      for (long long a = a0; a < b1; a += 4) {
         int32_t u[4];
+        if (p.col_vec) {
+          const int4 c4 = __ldg(col4 + (a >> 2));
+          u[0] = c4.x; u[1] = c4.y; u[2] = c4.z; u[3] = c4.w;
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; i++) u[i] = a + i < b1 ? __ldg(p.col + a + i) : 0;
+        }
         bool f[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++) u[i] = (e + i < b1) ? p.col[e + i] : -1;
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-          f[i] = u[i] >= 0 && ((__ldcg(front + (u[i] >> 5)) >> (u[i] & 31)) & 1u);
+        for (int i = 0; i < 4; i++) {
+          const bool in = (a + i >= b0) && (a + i < b1);
+          f[i] = in && (!p.bu_filter || ((__ldcg(front + (u[i] >> 5)) >> (u[i] & 31)) & 1u));
+        }
         uint32_t x[4][WORDS];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
@@ -750,7 +762,7 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
         for (int k = 0; k < WORDS; k++) x[k] = 0;
         if (e + lane < e_lim) {
           const int32_t u = p.col[e + lane];
-          if ((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u)
+          if (!p.bu_filter || ((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u))
             ld_status<WORDS>(gb.last + (size_t)u * WORDS, x);
         }
         miss = false;

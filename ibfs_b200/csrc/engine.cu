@@ -545,6 +545,8 @@ extern "C" void ibfs_opts_default(ibfs_opts* o) {
   o->timeout_ms = 0;
   o->max_levels = 0;
   o->debug_withhold = 0;
+  o->occupancy = 0;
+  o->bu_filter = -1;  // default: off (measured faster on B200)
 }
 
 static ibfs_status upload_graph(ibfs_graph* g) {
@@ -554,7 +556,9 @@ static ibfs_status upload_graph(ibfs_graph* g) {
   g->sms = sms;
   ibfs_status s;
   if ((s = g->beg.ensure(sizeof(int64_t) * (size_t)(g->V + 1))) != IBFS_OK) return s;
-  if ((s = g->col.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(g->E, 1))) != IBFS_OK) return s;
+  // + 4 entries: the bottom-up reads column ids as aligned 16-byte vectors
+  if ((s = g->col.ensure(sizeof(int32_t) * (size_t)(g->E + 4))) != IBFS_OK) return s;
+  CU(cudaMemset(g->col.p, 0, sizeof(int32_t) * (size_t)(g->E + 4)));
   CU(cudaStreamCreateWithFlags(&g->own_stream, cudaStreamNonBlocking));
   g->stream = g->own_stream;
   CU(cudaEventCreate(&g->ev0));
@@ -942,6 +946,8 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   p.lrec_cap = kLrecCap;
   p.vec_out = (rp.C % 4 == 0) && ((reinterpret_cast<uintptr_t>(dout) & 3) == 0);
   p.hub_t = kHubScan;
+  p.bu_filter = o.bu_filter > 0 ? 1 : 0;
+  p.col_vec = 1;
   p.vec_sm = (g->V % 4 == 0) && ((reinterpret_cast<uintptr_t>(dout) & 3) == 0);
 
   int64_t launches = 0;

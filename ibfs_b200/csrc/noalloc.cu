@@ -175,6 +175,8 @@ extern "C" ibfs_status ibfs_run_static_scratch(const int64_t* beg_dev, const int
   p.lrec_cap = kLrecCap;
   p.vec_out = ((reinterpret_cast<uintptr_t>(depth_dev) & 3) == 0) ? 1 : 0;
   p.hub_t = INT32_MAX;  // no deferred hub chunks here: the sweep scans whole lists
+  p.bu_filter = 0;
+  p.col_vec = 0;  // the caller's col is neither known to be padded nor aligned
   p.vec_sm = 0;
   NA_CU(launch_persistent_params(p, words, p.cpg, threads, 0, s));
 

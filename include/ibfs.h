@@ -95,7 +95,11 @@ typedef struct ibfs_opts {
     int32_t occupancy;     /* persistent kernel register budget / warps per SM:
                               0: 512 threads x 2 CTAs (64 regs), 1: 256 x 6 (42),
                               2: 256 x 8 (32), 3: 512 x 1 (128)                 */
-    int32_t reserved[6];
+    int32_t bu_filter;     /* bottom-up reads a neighbour's status only when the
+                              previous frontier bitmap has it: 1 on, 0 or -1 off
+                              (the default: the bitmap lookup costs more than the
+                              status reads it saves)                              */
+    int32_t reserved[5];
 } ibfs_opts;
 
 typedef struct ibfs_level_rec {
