@@ -416,36 +416,50 @@ static const void* persistent_for(int words, int level = 0) {
   }
 }
 
+// Plain schedule: every kernel gets as many CTAs as fit on the GPU for its
+// own register and shared-memory use (a grid-stride team over the whole grid).
+static int occ_grid(const void* fn, int threads, int sms) {
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, 0) != cudaSuccess) {
+    (void)cudaGetLastError();
+    per = 1;
+  }
+  return sms * std::max(per, 1);
+}
+
 template <int WORDS>
-static cudaError_t launch_plain_level(const Params& p, const GroupBufs& gb, int grid, int threads,
+static cudaError_t launch_plain_level(const Params& p, const GroupBufs& gb, int sms, int threads,
                                       int level, int dir, cudaStream_t s) {
   if (dir == kDirTD) {
-    k_qbuild<<<grid, threads, 0, s>>>(p, gb, level);
-    k_td<WORDS><<<grid, threads, 0, s>>>(p, gb, level);
+    k_qbuild<<<occ_grid((const void*)k_qbuild, threads, sms), threads, 0, s>>>(p, gb, level);
+    k_td<WORDS><<<occ_grid((const void*)k_td<WORDS>, threads, sms), threads, 0, s>>>(p, gb, level);
   } else {
-    k_bu<WORDS><<<grid, threads, 0, s>>>(p, gb, level);
-    k_bu_defer<WORDS><<<grid, threads, 0, s>>>(p, gb, level);
+    k_bu<WORDS><<<occ_grid((const void*)k_bu<WORDS>, threads, sms), threads, 0, s>>>(p, gb, level);
+    k_bu_defer<WORDS><<<occ_grid((const void*)k_bu_defer<WORDS>, threads, sms), threads, 0, s>>>(
+        p, gb, level);
   }
   return cudaGetLastError();
 }
 
 template <int WORDS>
-static cudaError_t launch_plain_inspect(const Params& p, const GroupBufs& gb, int grid, int threads,
+static cudaError_t launch_plain_inspect(const Params& p, const GroupBufs& gb, int sms, int threads,
                                         int b, int level, int dense, cudaStream_t s) {
-  k_inspect<WORDS><<<grid, threads, 0, s>>>(p, gb, b, level, dense);
+  k_inspect<WORDS><<<occ_grid((const void*)k_inspect<WORDS>, threads, sms), threads, 0, s>>>(
+      p, gb, b, level, dense);
   return cudaGetLastError();
 }
 
 template <int WORDS>
-static cudaError_t launch_plain_seed(const Params& p, int grid, int threads, int b, cudaStream_t s) {
-  k_seed<WORDS><<<grid, threads, 0, s>>>(p, b);
+static cudaError_t launch_plain_seed(const Params& p, int sms, int threads, int b, cudaStream_t s) {
+  k_seed<WORDS><<<sms, threads, 0, s>>>(p, b);
   return cudaGetLastError();
 }
 
 template <int WORDS>
-static cudaError_t launch_plain_output(const Params& p, const GroupBufs& gb, int grid, int threads,
+static cudaError_t launch_plain_output(const Params& p, const GroupBufs& gb, int sms, int threads,
                                        int b, int max_level, cudaStream_t s) {
-  k_output<WORDS><<<grid, threads, 0, s>>>(p, gb, b, max_level);
+  k_output<WORDS><<<occ_grid((const void*)k_output<WORDS>, threads, sms), threads, 0, s>>>(
+      p, gb, b, max_level);
   return cudaGetLastError();
 }
 
@@ -1035,7 +1049,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     CU(cudaMemsetAsync(g->d_brec.p, 0, sizeof(BatchRec) * rp.nbatches, s));
     CU(cudaEventRecord(g->ev0, s));
     const GroupBufs gb = hgb[0];
-    const int grid = rp.grid, thr = rp.threads;
+    const int grid = g->sms, thr = rp.threads;  // launch helpers size each grid
     Par* hpar = reinterpret_cast<Par*>(g->h_par.p);
     BatchRec* hbr = g->h_brec.as<BatchRec>();
     LevelRec* hlr = g->h_lrec.as<LevelRec>();
