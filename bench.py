@@ -3,8 +3,9 @@
 Default workload: R-MAT scale 24 (16.8M vertices, edge factor 16, a/b/c/d =
 .57/.19/.19/.05, ~537M directed CSR entries), 1024 sources from the giant
 component, GroupBy into 8 batches of 128 sources with 128-bit status words,
-one persistent launch per run replayed from a CUDA graph.  A step is one
-whole run over all 1024 sources.
+run by the device-loop schedule: one CUDA graph launch per run whose
+conditional nodes drive the batch and level loops over one kernel per phase,
+4 batches concurrently.  A step is one whole run over all 1024 sources.
 
   value   aggregate GTEPS (sum over sources of the edges of the vertices each
           source reached, validate.h:59-76, / device time) with the CSR and the
@@ -13,16 +14,20 @@ whole run over all 1024 sources.
           uploaded from pinned memory and every depth byte copied back to
           pinned host memory inside the timed region;
   roofline: algorithmic bytes of the run (the implementation-independent byte
-          model, computed on the GPU from the depths) / the persistent kernel's
-          average event-timed duration, against MEASURED_PEAKS.json hbm_gbs.
+          model, computed on the GPU from the depths) / the run's average
+          event-timed device duration (the one graph launch: every phase
+          kernel of the run), against MEASURED_PEAKS.json hbm_gbs; the
+          per-phase split comes from the kernels' %globaltimer stamps.
 
 ``--impl reference`` times the CPU oracle (the project's restatement of the
 reference's sequential BFS; the reference has no runnable CPU BFS of its own)
 on all host cores over a bounded sample of the same workload.
 
-Multi-GPU (torchrun): sources shard across ranks -- every rank runs its own
-1024 sources on a full replica of the graph, no collective on the data path
-(weak scaling); timing is the max over ranks.
+Multi-GPU (torchrun): sources shard across ranks as in the reference's MPI
+build -- rank 0 builds the graph and broadcasts the replica, the N*1024
+global sources are GroupBy-ordered and every rank takes its contiguous block
+(ibfs_b200.shard); no collective on the data path (weak scaling); timing is
+the max over ranks.
 """
 from __future__ import annotations
 
@@ -235,16 +240,32 @@ def run_ours(args, cfg):
     torch.cuda.set_device(local)
     torch.cuda.init()
     t_gen = time.perf_counter()
-    beg, col = make_graph(cfg)
-    src = ib.sample_sources(beg, col, cfg["nsrc"], cfg["src_seed"] + 1000 * rank,
-                            giant_component=cfg["giant"])
+    if world == 1:
+        beg, col = make_graph(cfg)
+        src = ib.sample_sources(beg, col, cfg["nsrc"], cfg["src_seed"],
+                                giant_component=cfg["giant"])
+    else:
+        # Source sharding as the reference's MPI build: rank 0 builds the graph
+        # and broadcasts the replica, the N*nsrc global sources are GroupBy-
+        # ordered and every rank takes its contiguous block (weak scaling).
+        from ibfs_b200 import shard
+
+        if rank == 0:
+            beg, col = shard.replicate_csr(*make_graph(cfg))
+        else:
+            beg, col = shard.replicate_csr()
+        glb = ib.sample_sources(beg, col, cfg["nsrc"] * world, cfg["src_seed"],
+                                giant_component=cfg["giant"])
+        order = glb if args.no_groupby else ib.groupby_csr(beg, col, glb)
+        src = shard.arrange_src(order, world, rank)
     t_gen = time.perf_counter() - t_gen
     V = len(beg) - 1
     g = ib.Graph.from_csr(beg, col, device=local)
     stream = torch.cuda.Stream(device=local)
     g.set_stream(stream.cuda_stream)
     opts = ib.default_opts(width=args.width, concurrent=args.concurrent,
-                           mode=ib.MODE_PERSISTENT if args.mode == "persistent" else ib.MODE_PLAIN,
+                           mode={"devloop": ib.MODE_DEVICE_LOOP, "persistent": ib.MODE_PERSISTENT,
+                                 "plain": ib.MODE_PLAIN}[args.mode],
                            groupby=0 if args.no_groupby else 1, use_graph=0 if args.no_graph else 1,
                            depth_bytes=1, groups=args.groups)
     n = len(src)
@@ -296,6 +317,24 @@ def run_ours(args, cfg):
             total += g.bytes_alg(blk.data_ptr(), blk.shape[0], 1, args.width)
             del blk
         bytes_alg = total
+    # ---- per-phase device time of one (untimed) run, from the level records
+    phases = None
+    if not args.no_roofline and args.mode != "plain":
+        rr = g.run(src, opts, on_device=True, out_ptr=out.data_ptr(), levels_cap=4096)
+        agg = {"td_expand": 0, "td_inspect": 0, "bu_expand": 0, "bu_inspect": 0, "output": 0,
+               "seed": 0}
+        for r in rr.levels:
+            if r["dir"] == 0:
+                agg["td_expand"] += r["expand_ns"]; agg["td_inspect"] += r["inspect_ns"]
+            elif r["dir"] == 1:
+                agg["bu_expand"] += r["expand_ns"]; agg["bu_inspect"] += r["inspect_ns"]
+            elif r["dir"] == 2:
+                agg["output"] += r["expand_ns"]
+            else:
+                agg["seed"] += r["expand_ns"] + r["inspect_ns"]
+        phases = {k: round(v / 1e6, 3) for k, v in agg.items()}
+        phases["note"] = ("sums over batches of %globaltimer spans; concurrent batches "
+                          "overlap, so the sum can exceed the run time")
     pk, pk_kind = peaks()
     roof = None
     if bytes_alg is not None:
@@ -312,7 +351,10 @@ def run_ours(args, cfg):
                 "peak_source": f"{pk_kind} MEASURED_PEAKS.json hbm_gbs" if pk_kind == "measured"
                 else "fallback 6650 GB/s",
                 "bytes_alg_per_launch": bytes_alg, "kernel_ms": round(kernel_ms, 4),
-                "kernel": "persistent_kernel<4>" if args.width == 128 else f"persistent_kernel(W={args.width})"}
+                "kernel": {"devloop": "device-loop graph (k_dl_* phase kernels, one launch per run)",
+                           "persistent": f"persistent_kernel (W={args.width})",
+                           "plain": "plain phase kernels"}[args.mode],
+                "phase_ms": phases}
 
     # ---- e2e: host buffers through the C ABI
     e2e = None
@@ -368,7 +410,10 @@ def run_ours(args, cfg):
             "data": "synthetic (seeded generators, no dataset)",
             "config": {"workload": cfg["workload"], "V": V, "E": int(len(col)), "sources": n,
                        "width": args.width, "concurrent": args.concurrent or args.width,
-                       "schedule": args.mode + ("+cuda-graph" if not args.no_graph else ""),
+                       "schedule": args.mode + ("+cuda-graph" if args.mode == "devloop" or
+                                                (args.mode == "persistent" and not args.no_graph)
+                                                else ""),
+                       "groups_requested": args.groups,
                        "groupby": not args.no_groupby, "parallelism": f"source-shard x{world}",
                        "l2": "inputs larger than L2 (CSR 2.1 GB, status 268 MB/batch)",
                        "gen_s": round(t_gen, 1), "max_level": res.stats["max_level"],
@@ -436,7 +481,7 @@ def main():
     ap.add_argument("--width", type=int, default=128)
     ap.add_argument("--concurrent", type=int, default=128)
     ap.add_argument("--groups", type=int, default=0)
-    ap.add_argument("--mode", default="persistent", choices=["persistent", "plain"])
+    ap.add_argument("--mode", default="devloop", choices=["devloop", "persistent", "plain"])
     ap.add_argument("--no-groupby", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

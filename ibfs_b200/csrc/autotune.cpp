@@ -1,11 +1,13 @@
 // autotune.cpp -- per-graph tuning of the traversal options.
 //
 // Coordinate descent over the knobs of one run: status width W (32, 64,
-// 128, 256 bits; batches of W sources), the small/large queue degree
-// thresholds, the CTA size, the direction-switch alpha/beta and the number
-// of concurrently running batches.  Every trial is the real persistent run
-// on the caller's sample of sources with the depths left on the device; the
-// score is aggregate traversed edges per device second.  The reference has
+// 128, 256 bits; batches of W sources), the direction-switch alpha/beta, the
+// small/large queue degree thresholds, the persistent kernel's occupancy
+// level (persistent schedule only) and the number of concurrently running
+// batches.  Every trial is the real run, in the base options' schedule
+// (device loop or persistent kernel), on the caller's sample of sources with
+// the depths left on the device; the score is aggregate traversed edges per
+// device second.  The reference has
 // no tuner (its constants are fixed: comm.h:25-30, ibfs.cu:71-72).
 #include <algorithm>
 #include <cstdio>
@@ -52,7 +54,8 @@ extern "C" ibfs_status ibfs_autotune(ibfs_graph* g, const int32_t* src, int64_t 
   ibfs_opts o0;
   if (base) o0 = *base;
   else ibfs_opts_default(&o0);
-  o0.mode = IBFS_MODE_PERSISTENT;
+  if (o0.mode == IBFS_MODE_PLAIN) o0.mode = IBFS_MODE_DEVICE_LOOP;  // no host loop in trials
+  const bool persistent = o0.mode == IBFS_MODE_PERSISTENT;
   o0.use_graph = 1;
   if (o0.depth_bytes == 0) o0.depth_bytes = 1;
   if (reps < 1) reps = 2;
@@ -101,7 +104,9 @@ extern "C" ibfs_status ibfs_autotune(ibfs_graph* g, const int32_t* src, int64_t 
   const float betas[] = {8.0f, 24.0f, 64.0f, 256.0f};
   const int thr[][2] = {{16, 256}, {32, 512}, {64, 1024}, {32, 4096}, {8, 128}};
   const int occ[] = {0, 1, 2};
-  const int groups[] = {0, 1, 2, 4};
+  const int groups_p[] = {0, 1, 2, 4};
+  const int groups_d[] = {1, 2, 4, 8};
+  const int* groups = persistent ? groups_p : groups_d;
   s = try_set([&](ibfs_opts& o, int i) {
         o.width = widths[i];
         o.concurrent = 0;
@@ -117,7 +122,7 @@ extern "C" ibfs_status ibfs_autotune(ibfs_graph* g, const int32_t* src, int64_t 
           o.lrg_shed = thr[i][1];
           return true;
         }, 5);
-  if (s == IBFS_OK)
+  if (s == IBFS_OK && persistent)
     s = try_set([&](ibfs_opts& o, int i) { o.occupancy = occ[i]; return true; }, 3);
   if (s == IBFS_OK)
     s = try_set([&](ibfs_opts& o, int i) { o.groups = groups[i]; return true; }, 4);

@@ -50,6 +50,22 @@ struct Par {
   int32_t pad[2];
 };
 
+// State of the level loop when it runs as kernels inside a CUDA graph (the
+// device-driven schedule): what the persistent kernel keeps in registers
+// lives here between kernels.
+struct LoopState {
+  long long n_total;  // sources of the run (set by the host before the launch)
+  int32_t nbatches;   // batches of the run (set by the host before the launch)
+  int32_t batch;      // batch the group is traversing
+  int32_t level;      // level being expanded / inspected
+  int32_t dir;        // direction of `level`
+  int32_t max_level;
+  int32_t td, bu;
+  int32_t err;
+  unsigned long long m_u, teps, prev_changed;
+  unsigned long long t_lvl, t_mid;  // %globaltimer at the level start / inspect start
+};
+
 // Control block of one group (one batch at a time).  256-byte aligned.
 struct __align__(256) Ctl {
   unsigned int bar_count;
@@ -59,6 +75,7 @@ struct __align__(256) Ctl {
   Par par[2];
   int32_t qc[2][4];  // [consumer level parity][small, medium, large-chunks]
   unsigned long long pad1[4];
+  LoopState ls;
 };
 
 struct BatchRec {
@@ -283,18 +300,25 @@ __device__ __forceinline__ void zero_words(uint32_t* p, long long nwords, const 
 //   fixed (switch_level >= 0): top-down while level <= switch_level, then
 //     bottom-up -- the reference's CLI switch level (expander.cuh:687-723);
 //   alpha/beta (Beamer et al., SC'12): top-down -> bottom-up when the
-//     frontier's edges exceed unexplored_edges/alpha; bottom-up -> top-down
-//     when the frontier holds fewer than V/beta vertices.
+//     frontier's edges exceed unexplored_edges/alpha and the frontier is
+//     growing; bottom-up -> top-down when the frontier holds fewer than
+//     V/beta vertices and is shrinking.  Without the growing/shrinking
+//     tests a long shrinking tail (high-diameter graphs) flips direction
+//     every level once the unexplored edges run low, paying a full
+//     bottom-up sweep for a handful of frontier vertices.
 // ---------------------------------------------------------------------------
 __host__ __device__ inline int choose_dir(int next_level, int prev_dir,
                                           int switch_level, float alpha,
                                           float beta, unsigned long long changed,
+                                          unsigned long long prev_changed,
                                           unsigned long long mf,
                                           unsigned long long m_u, long long V) {
   if (switch_level >= 0) return next_level <= switch_level ? kDirTD : kDirBU;
   if (prev_dir == kDirTD)
-    return ((double)mf * (double)alpha > (double)m_u) ? kDirBU : kDirTD;
-  return ((double)changed * (double)beta < (double)V) ? kDirTD : kDirBU;
+    return ((double)mf * (double)alpha > (double)m_u && changed > prev_changed) ? kDirBU
+                                                                                : kDirTD;
+  return ((double)changed * (double)beta < (double)V && changed < prev_changed) ? kDirTD
+                                                                                : kDirBU;
 }
 
 // ---------------------------------------------------------------------------
@@ -352,26 +376,52 @@ __device__ __forceinline__ void inspect_vertex(const Params& p, const GroupBufs&
   if (comp) cdeg += deg;
   if (depth_ok) {
     // depth(v, s) = level for the new bits: OR them into the planes of the
-    // level's set bits (one coalesced read-modify-write per plane).
-    for (int b = 0; (level >> b) != 0; b++) {
-      if (!((level >> b) & 1)) continue;
-      uint32_t* q = gb.planes + (size_t)b * p.plane_stride + (size_t)v * WORDS;
-      uint32_t x[WORDS];
-      ld_status<WORDS>(q, x);
+    // level's set bits (one coalesced read-modify-write per plane), two
+    // planes at a time so that their loads are in flight together.
+    uint32_t* q0 = gb.planes + (size_t)v * WORDS;
+    unsigned rest = (unsigned)level;
+    while (rest) {
+      const int b0 = __ffs(rest) - 1;
+      rest &= rest - 1;
+      uint32_t* qa = q0 + (size_t)b0 * p.plane_stride;
+      uint32_t xa[WORDS];
+      ld_status<WORDS>(qa, xa);
+      if (rest) {
+        const int b1 = __ffs(rest) - 1;
+        rest &= rest - 1;
+        uint32_t* qb = q0 + (size_t)b1 * p.plane_stride;
+        uint32_t xb[WORDS];
+        ld_status<WORDS>(qb, xb);
 #pragma unroll
-      for (int k = 0; k < WORDS; k++) x[k] |= nb[k];
-      st_status<WORDS>(q, x);
+        for (int k = 0; k < WORDS; k++) xb[k] |= nb[k];
+        st_status<WORDS>(qb, xb);
+      }
+#pragma unroll
+      for (int k = 0; k < WORDS; k++) xa[k] |= nb[k];
+      st_status<WORDS>(qa, xa);
     }
   }
 }
 
 // ---------------------------------------------------------------------------
 // Phase: inspect level L (reads the level-L bitmap, fixes last, updates the
-// depth bit-planes, counters).  `dense` picks the walk: one bitmap word per
-// warp step spread over all warps (many changed vertices), or 128 words per
-// warp step with only the non-empty words visited (few changed vertices).
+// depth bit-planes, counters).  Every warp step takes 32 bitmap words (1024
+// vertices) and compacts their set bits across the warp: lane j of round k
+// inspects the (32k + j)-th changed vertex of the chunk, found by a binary
+// search over the warp's inclusive bit counts (per-lane shuffles) and
+// __fns within the owning word.  All 32 lanes work on a changed vertex in
+// every full round whatever the density or the spread of the changed set,
+// so a frontier scattered thinly over the whole graph (a grid late in a
+// traversal, a power-law graph's tail) costs rounds of 32 vertices, not
+// one mostly idle round per non-empty word.
+//
+// LEAN selects the walk of the persistent kernel instead, whose budget of
+// 64 registers per thread (2 x 512 threads per SM) has no room for the
+// compaction: lanes map to the bits of one word, one word per warp step
+// (`dense`, many changed vertices) or the non-empty words of 128-word
+// blocks (few changed vertices).
 // ---------------------------------------------------------------------------
-template <int WORDS>
+template <int WORDS, bool LEAN>
 __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par, int n_b,
                               int level, bool depth_ok, bool dense, const Team& t) {
   uint32_t full[WORDS];
@@ -386,7 +436,7 @@ __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par, in
   // bottom-up merges into it with atomics
   zero_words(chg_at(gb, p, level + 1), p.chg_stride, t);
   const int lane = t.lane;
-  if (dense) {
+  if (LEAN && dense) {
     for (long long w = t.warp; w < p.nchg; w += t.nwarps) {
       const uint32_t bits = __ldcg(chg + w);
       if (!bits) continue;
@@ -394,7 +444,7 @@ __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par, in
       if ((bits >> lane) & 1u)
         inspect_vertex<WORDS>(p, gb, v, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
     }
-  } else {
+  } else if (LEAN) {
     const long long nblk = (p.nchg + 127) / 128;
     for (long long blk = t.warp; blk < nblk; blk += t.nwarps) {
       const uint4 q4 = __ldcg(reinterpret_cast<const uint4*>(chg) + blk * 32 + lane);
@@ -417,6 +467,38 @@ __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par, in
           inspect_vertex<WORDS>(p, gb, (w0 + 3) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
       }
     }
+  } else {
+  const long long nchunk = (p.nchg + 31) / 32;  // whole chunks lie inside chg_stride
+  for (long long c = t.warp; c < nchunk; c += t.nwarps) {
+    const uint32_t word = __ldcg(chg + c * 32 + lane);
+    if (__ballot_sync(0xFFFFFFFFu, word != 0u) == 0u) continue;
+    const int own = __popc(word);
+    int incl = own;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int excl = incl - own;
+    const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    for (int base = 0; base < total; base += 32) {
+      const int r = base + lane;
+      // owner = number of lanes whose inclusive count is <= r
+      int lo = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        const int probe = __shfl_sync(0xFFFFFFFFu, incl, lo + step - 1);
+        if (probe <= r) lo += step;
+      }
+      const uint32_t w = __shfl_sync(0xFFFFFFFFu, word, lo);
+      const int e = __shfl_sync(0xFFFFFFFFu, excl, lo);
+      if (r < total) {
+        const int bit = (int)__fns(w, 0u, r - e + 1);
+        const long long v = (c * 32 + lo) * 32 + bit;
+        inspect_vertex<WORDS>(p, gb, v, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
+      }
+    }
+  }
   }
   if (!depth_ok && cnt) par->range_err = 1;
   cta_add_u64(&par->changed, cnt);
@@ -427,7 +509,7 @@ __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par, in
   for (int k = 0; k < WORDS; k++) cta_or_u32(&par->fmask[k], fm[k]);
 }
 
-// Whether the inspect of the next level should use the dense walk: its
+// Whether the lean inspect of the next level should use the dense walk: its
 // changed set is at most the previous frontier's neighbourhood.
 __host__ __device__ inline bool inspect_dense(unsigned long long prev_mf, long long V) {
   return prev_mf * 16ull > (unsigned long long)V;

@@ -22,6 +22,8 @@
 //   --thresholds S,L   degree thresholds of the small/large queues (32,512)
 //   --groupby          reorder sources with GroupBy before batching
 //   --plain            host-driven level loop (default: persistent kernel)
+//   --device-loop      kernel per phase, level loop on the device (CUDA graph
+//                      conditional nodes)
 //   --batched          all batches in one launch (CUDA graph), one report
 //   --repeat K         run the whole set K times (timing)
 //   --device D, --seed S, --depth-bytes 1|2, --vertex-major
@@ -37,7 +39,7 @@
 static void usage() {
   std::printf("Input: /path/to/exe /path/to/beg /path/to/csr concurrent-count switch-level "
               "bfs_count [--sources F] [--depth-out F] [--width W] [--alpha A] [--beta B] "
-              "[--thresholds S,L] [--groupby] [--plain] [--batched] [--repeat K] [--device D] "
+              "[--thresholds S,L] [--groupby] [--plain] [--device-loop] [--batched] [--repeat K] [--device D] "
               "[--seed S] [--depth-bytes 1|2] [--vertex-major]\n");
 }
 
@@ -86,6 +88,7 @@ int main(int argc, char** argv) {
       }
     } else if (a == "--groupby") o.groupby = 1;
     else if (a == "--plain") o.mode = IBFS_MODE_PLAIN;
+    else if (a == "--device-loop") o.mode = IBFS_MODE_DEVICE_LOOP;
     else if (a == "--batched") batched = true;
     else if (a == "--repeat") repeat = std::atoi(next("--repeat"));
     else if (a == "--device") device = std::atoi(next("--device"));

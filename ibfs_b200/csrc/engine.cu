@@ -90,10 +90,10 @@ __global__ void __launch_bounds__(THREADS, MINB) persistent_kernel(Params p) {
     BARRIER();
     seed_phase<WORDS>(p, gb, p.src + k0, n_b, t);
     BARRIER();
-    inspect_phase<WORDS>(p, gb, &ctl->par[0], n_b, 0, true, false, t);
+    inspect_phase<WORDS, true>(p, gb, &ctl->par[0], n_b, 0, true, false, t);
     BARRIER();
     int level = 0, cur_dir = kDirTD, max_level = 0, td = 0, bu = 0;
-    unsigned long long m_u = (unsigned long long)p.E, teps = 0;
+    unsigned long long m_u = (unsigned long long)p.E, teps = 0, prev_changed = 0;
     unsigned long long t_lvl = global_ns(), t_mid = t_lvl;
     int err = 0;
     while (true) {
@@ -108,7 +108,8 @@ __global__ void __launch_bounds__(THREADS, MINB) persistent_kernel(Params p) {
         else if (level + 1 > p.max_levels) { stop = 1; err = 3; }
         if (changed && !pr->range_err) max_level = level;
         const int nd = choose_dir(level + 1, cur_dir, p.switch_level, p.alpha, p.beta,
-                                  changed, mf, m_u, p.V);
+                                  changed, prev_changed, mf, m_u, p.V);
+        prev_changed = changed;
         if (t.block == 0) {
           if (level < p.lrec_cap) {
             LevelRec r;
@@ -133,9 +134,9 @@ __global__ void __launch_bounds__(THREADS, MINB) persistent_kernel(Params p) {
       }
       __syncthreads();
       const int stop = s_stop;
-      const bool dense = s_dense != 0;
       cur_dir = s_dir;
       err = s_err;
+      const bool dense = s_dense != 0;
       __syncthreads();
       if (stop) break;
       level++;
@@ -163,8 +164,8 @@ __global__ void __launch_bounds__(THREADS, MINB) persistent_kernel(Params p) {
         BARRIER();
         if (lead) t_mid = global_ns();
       }
-      inspect_phase<WORDS>(p, gb, &ctl->par[level & 1], n_b, level,
-                           level <= depth_limit(p.db), dense, t);
+      inspect_phase<WORDS, true>(p, gb, &ctl->par[level & 1], n_b, level,
+                                 level <= depth_limit(p.db), dense, t);
       BARRIER();
     }
     if (err) {
@@ -210,13 +211,12 @@ __global__ void __launch_bounds__(512) k_seed(Params p, int b) {
 }
 
 template <int WORDS>
-__global__ void __launch_bounds__(512) k_inspect(Params p, GroupBufs gb, int b, int level,
-                                                 int dense) {
+__global__ void __launch_bounds__(512) k_inspect(Params p, GroupBufs gb, int b, int level) {
   const Team t = make_team(blockIdx.x, gridDim.x);
   const long long k0 = (long long)b * p.C;
   const int n_b = (int)min((long long)p.C, p.n_total - k0);
-  inspect_phase<WORDS>(p, gb, &gb.ctl->par[level & 1], n_b, level, level <= depth_limit(p.db),
-                       dense != 0, t);
+  inspect_phase<WORDS, false>(p, gb, &gb.ctl->par[level & 1], n_b, level,
+                              level <= depth_limit(p.db), false, t);
 }
 
 __global__ void __launch_bounds__(512) k_qbuild(Params p, GroupBufs gb, int level) {
@@ -254,6 +254,200 @@ __global__ void __launch_bounds__(512) k_output(Params p, GroupBufs gb, int b, i
   output_phase<WORDS>(p, gb, batch_depth(p, b), s_rows, n_b, max_level, t);
 }
 
+// ---- device-driven schedule ------------------------------------------------
+// The plain schedule's kernels inside one CUDA graph whose conditional nodes
+// run the batch loop (WHILE) and the level loop (WHILE, with a SWITCH on the
+// direction), so that every phase keeps the register budget and occupancy of
+// its own kernel while no level needs a host round trip.  The batch and the
+// level come from the group's LoopState; the decision kernel is the
+// persistent kernel's top-of-level block (same rule, same records) run by one
+// thread.  All kernels share one signature so that the graph builder can
+// bind them uniformly: (params, group, handle 0, handle 1).
+using CondH = cudaGraphConditionalHandle;
+
+// The run's source and batch counts come from the control block, not from
+// Params, so that one built graph serves runs of any size.
+__device__ __forceinline__ int dl_batch_size(const Params& p, const LoopState& ls, int b) {
+  return (int)min((long long)p.C, ls.n_total - (long long)b * p.C);
+}
+
+// First batch of group g; the batch loop runs while it exists.
+__global__ void k_dl_start(Params p, int g, CondH h_batch, CondH) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Ctl* ctl = p.groups[g].ctl;
+  ctl->ls.batch = g;
+  ctl->ls.err = 0;
+  cudaGraphSetConditional(h_batch, g < ctl->ls.nbatches ? 1u : 0u);
+}
+
+// Zero the group's status words and bitmaps, reset the counters and the
+// loop state for the batch; arm the level loop.
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_dl_batch_init(Params p, int g, CondH h_level, CondH) {
+  const GroupBufs gb = p.groups[g];
+  const Team t = make_team(blockIdx.x, gridDim.x);
+  const long long vpad = (p.V + 31) & ~31LL;
+  zero_words(gb.last, vpad * WORDS, t);
+  zero_words(gb.curr, vpad * WORDS, t);
+  zero_words(gb.chg, 2 * p.chg_stride, t);
+  if (t.tid == 0) {
+    Ctl* ctl = gb.ctl;
+    memset(&ctl->par[0], 0, sizeof(Par) * 2);
+    memset(&ctl->qc[0][0], 0, sizeof(ctl->qc));
+    LoopState& ls = ctl->ls;
+    ls.level = 0;
+    ls.dir = kDirTD;
+    ls.max_level = 0;
+    ls.td = ls.bu = 0;
+    ls.m_u = (unsigned long long)p.E;
+    ls.teps = 0;
+    ls.prev_changed = 0;
+    ls.t_lvl = ls.t_mid = global_ns();
+    cudaGraphSetConditional(h_level, 1u);
+  }
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_dl_seed(Params p, int g, CondH, CondH) {
+  const GroupBufs gb = p.groups[g];
+  const int b = gb.ctl->ls.batch;
+  seed_phase<WORDS>(p, gb, p.src + (long long)b * p.C, dl_batch_size(p, gb.ctl->ls, b),
+                    make_team(blockIdx.x, gridDim.x));
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_dl_inspect(Params p, int g, CondH, CondH) {
+  const GroupBufs gb = p.groups[g];
+  Ctl* ctl = gb.ctl;
+  const int b = ctl->ls.batch, level = ctl->ls.level;
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ls.t_mid = global_ns();
+  inspect_phase<WORDS, false>(p, gb, &ctl->par[level & 1], dl_batch_size(p, ctl->ls, b), level,
+                              level <= depth_limit(p.db), false, make_team(blockIdx.x, gridDim.x));
+}
+
+// Top of a level: read the counters of the level just inspected, stop or
+// pick the next direction (choose_dir), write the level record, advance.
+// h_level keeps the level loop running, h_dir selects the expand body
+// (0 top-down, 1 bottom-up, 2 none: the loop ends).
+__global__ void k_dl_decide(Params p, int g, CondH h_level, CondH h_dir) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Ctl* ctl = p.groups[g].ctl;
+  LoopState& ls = ctl->ls;
+  const int level = ls.level, b = ls.batch;
+  const Par& pr = ctl->par[level & 1];
+  const unsigned long long changed = pr.changed, mf = pr.mf, cdeg = pr.cdeg;
+  ls.teps += pr.teps;
+  ls.m_u = ls.m_u > cdeg ? ls.m_u - cdeg : 0ull;
+  int stop = 0, err = 0;
+  if (pr.range_err) { stop = 1; err = 3; }
+  else if (changed == 0) stop = 1;
+  else if (level + 1 > p.max_levels) { stop = 1; err = 3; }
+  if (changed && !pr.range_err) ls.max_level = level;
+  const int nd = choose_dir(level + 1, ls.dir, p.switch_level, p.alpha, p.beta, changed,
+                            ls.prev_changed, mf, ls.m_u, p.V);
+  ls.prev_changed = changed;
+  const unsigned long long t_now = global_ns();
+  if (level < p.lrec_cap) {
+    LevelRec r;
+    r.batch = b; r.level = level; r.dir = level == 0 ? -1 : ls.dir; r.pad = 0;
+    r.frontier = (long long)changed; r.frontier_edges = (long long)mf;
+    r.expand_ns = (long long)(ls.t_mid - ls.t_lvl);
+    r.inspect_ns = (long long)(t_now - ls.t_mid);
+    p.lrec[(size_t)b * p.lrec_cap + level] = r;
+  }
+  ls.t_lvl = t_now;
+  ls.err = err;
+  if (!stop) {
+    memset((void*)&ctl->par[(level + 1) & 1], 0, sizeof(Par));
+    ctl->qc[level & 1][0] = ctl->qc[level & 1][1] = ctl->qc[level & 1][2] = 0;
+    ls.dir = nd;
+    ls.level = level + 1;
+    if (nd == kDirTD) ls.td++; else ls.bu++;
+  }
+  cudaGraphSetConditional(h_level, stop ? 0u : 1u);
+  cudaGraphSetConditional(h_dir, stop ? 2u : (unsigned)nd);
+}
+
+__global__ void __launch_bounds__(512) k_dl_qbuild(Params p, int g, CondH, CondH) {
+  const GroupBufs gb = p.groups[g];
+  const int level = gb.ctl->ls.level;
+  const Team t = make_team(blockIdx.x, gridDim.x);
+  zero_plane_if_first(p, gb, level, t);
+  qbuild_phase(p, gb, level, gb.ctl->qc[level & 1], t);
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_dl_td(Params p, int g, CondH, CondH) {
+  const GroupBufs gb = p.groups[g];
+  const int level = gb.ctl->ls.level;
+  td_phase<WORDS>(p, gb, level, gb.ctl->qc[level & 1], make_team(blockIdx.x, gridDim.x));
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_dl_bu(Params p, int g, CondH, CondH) {
+  const GroupBufs gb = p.groups[g];
+  const int level = gb.ctl->ls.level;
+  const Team t = make_team(blockIdx.x, gridDim.x);
+  zero_plane_if_first(p, gb, level, t);
+  bu_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
+                  &gb.ctl->par[level & 1].hq_cnt, t);
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_dl_bu_defer(Params p, int g, CondH, CondH) {
+  const GroupBufs gb = p.groups[g];
+  const int level = gb.ctl->ls.level;
+  if (gb.ctl->par[level & 1].hq_cnt == 0) return;  // uniform: nothing deferred
+  bu_defer_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
+                        &gb.ctl->par[level & 1].hq_cnt, make_team(blockIdx.x, gridDim.x));
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_dl_output(Params p, int g, CondH, CondH) {
+  __shared__ int32_t s_rows[kMaxWords * 32];
+  const GroupBufs gb = p.groups[g];
+  const LoopState& ls = gb.ctl->ls;
+  if (ls.err) return;  // uniform
+  const int b = ls.batch, n_b = dl_batch_size(p, ls, b);
+  load_rows(p, b, n_b, s_rows);
+  output_phase<WORDS>(p, gb, batch_depth(p, b), s_rows, n_b, ls.max_level,
+                      make_team(blockIdx.x, gridDim.x));
+}
+
+// End of a batch: its record (or the group's error), then the next batch of
+// the group; the batch loop ends after the last one or on an error.
+__global__ void k_dl_batch_end(Params p, int g, CondH h_batch, CondH) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Ctl* ctl = p.groups[g].ctl;
+  LoopState& ls = ctl->ls;
+  const int b = ls.batch;
+  if (ls.err) {
+    atomicCAS(&ctl->err, 0, ls.err);
+    p.brec[b].err = ls.err;
+    cudaGraphSetConditional(h_batch, 0u);
+    return;
+  }
+  if (ls.level + 1 < p.lrec_cap) {
+    LevelRec r;  // dir 2: the batch's output pass
+    r.batch = b; r.level = ls.level + 1; r.dir = 2; r.pad = 0;
+    r.frontier = 0; r.frontier_edges = 0;
+    r.expand_ns = (long long)(global_ns() - ls.t_lvl);
+    r.inspect_ns = 0;
+    p.lrec[(size_t)b * p.lrec_cap + ls.level + 1] = r;
+  }
+  BatchRec r;
+  r.levels = ls.level;
+  r.max_level = ls.max_level;
+  r.td = ls.td;
+  r.bu = ls.bu;
+  r.teps = ls.teps;
+  r.err = 0;
+  r.pad = 0;
+  p.brec[b] = r;
+  ls.batch = b + p.G;
+  cudaGraphSetConditional(h_batch, ls.batch < ls.nbatches ? 1u : 0u);
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -288,6 +482,13 @@ struct DevBuf {
     }
     bytes = std::max<size_t>(want, 256);
     return IBFS_OK;
+  }
+  // Small per-run buffers grow to powers of two so that their addresses
+  // (baked into cached CUDA graphs) stay put across runs of similar size.
+  ibfs_status ensure_pow2(size_t want) {
+    size_t r = 4096;
+    while (r < want) r <<= 1;
+    return want <= bytes && p ? IBFS_OK : ensure(r);
   }
   void release() {
     if (p) cudaFree(p);
@@ -357,6 +558,7 @@ struct ibfs_graph {
   DevBuf d_groups, d_src, d_outrow, d_brec, d_lrec, d_out;
   PinBuf h_src, h_outrow, h_brec, h_lrec, h_par;
   GraphCache gcache;
+  GraphCache dlcache;  // device-driven schedule: keyed by the launch Params
   std::mutex mu;
 };
 
@@ -370,7 +572,9 @@ static ibfs_status check_opts(const ibfs_opts* o) {
   if (o->width != 32 && o->width != 64 && o->width != 128 && o->width != 256)
     return IBFS_ERR_INVALID_ARG;
   if (o->concurrent < 0 || o->concurrent > o->width) return IBFS_ERR_INVALID_ARG;
-  if (o->mode != IBFS_MODE_PLAIN && o->mode != IBFS_MODE_PERSISTENT) return IBFS_ERR_INVALID_ARG;
+  if (o->mode != IBFS_MODE_PLAIN && o->mode != IBFS_MODE_PERSISTENT &&
+      o->mode != IBFS_MODE_DEVICE_LOOP)
+    return IBFS_ERR_INVALID_ARG;
   if (o->depth_bytes != 0 && o->depth_bytes != 1 && o->depth_bytes != 2) return IBFS_ERR_INVALID_ARG;
   if (o->threads != 0 && o->threads != 128 && o->threads != 256 && o->threads != 512)
     return IBFS_ERR_INVALID_ARG;
@@ -443,9 +647,9 @@ static cudaError_t launch_plain_level(const Params& p, const GroupBufs& gb, int 
 
 template <int WORDS>
 static cudaError_t launch_plain_inspect(const Params& p, const GroupBufs& gb, int sms, int threads,
-                                        int b, int level, int dense, cudaStream_t s) {
+                                        int b, int level, cudaStream_t s) {
   k_inspect<WORDS><<<occ_grid((const void*)k_inspect<WORDS>, threads, sms), threads, 0, s>>>(
-      p, gb, b, level, dense);
+      p, gb, b, level);
   return cudaGetLastError();
 }
 
@@ -468,6 +672,100 @@ static cudaError_t launch_plain_output(const Params& p, const GroupBufs& gb, int
    : (words) == 2 ? fn<2>(__VA_ARGS__)                  \
    : (words) == 4 ? fn<4>(__VA_ARGS__)                  \
                   : fn<8>(__VA_ARGS__))
+
+// ---- device-driven schedule: graph construction ------------------------
+using DlKernel = void (*)(Params, int, CondH, CondH);
+
+static cudaError_t dl_kernel(cudaGraph_t gr, cudaGraphNode_t* out, cudaGraphNode_t dep,
+                             DlKernel fn, int grid, int threads, const Params& p, int g,
+                             CondH h0, CondH h1) {
+  Params pp = p;
+  int gg = g;
+  CondH a = h0, b = h1;
+  void* args[] = {&pp, &gg, &a, &b};
+  cudaKernelNodeParams kp;
+  std::memset(&kp, 0, sizeof(kp));
+  kp.func = reinterpret_cast<void*>(fn);
+  kp.gridDim = dim3((unsigned)grid);
+  kp.blockDim = dim3((unsigned)threads);
+  kp.kernelParams = args;
+  return cudaGraphAddKernelNode(out, gr, dep ? &dep : nullptr, dep ? 1 : 0, &kp);
+}
+
+static cudaError_t dl_cond(cudaGraph_t gr, cudaGraphNode_t* out, cudaGraphNode_t dep, CondH h,
+                           cudaGraphConditionalNodeType type, unsigned size, cudaGraph_t* bodies) {
+  cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+  np.conditional.handle = h;
+  np.conditional.type = type;
+  np.conditional.size = size;
+  cudaError_t e = cudaGraphAddNode(out, gr, dep ? &dep : nullptr, dep ? 1 : 0, &np);
+  if (e == cudaSuccess)
+    for (unsigned i = 0; i < size; i++) bodies[i] = np.conditional.phGraph_out[i];
+  return e;
+}
+
+// One branch per group g:
+//   start -> WHILE(batch) { init -> seed -> inspect(0) -> WHILE(level) {
+//              decide -> SWITCH(dir) { 0: qbuild -> td -> inspect,
+//                                      1: bu -> bu_defer -> inspect } }
+//            -> output -> batch_end }
+// Every loop ends: decide stops at an empty level or past max_levels, and
+// batch_end stops after the group's last batch or on an error.
+template <int WORDS>
+static cudaError_t build_device_loop(const Params& p, int G, int sms, int threads,
+                                     cudaGraph_t* out) {
+  *out = nullptr;
+  cudaGraph_t top = nullptr;
+  cudaError_t e = cudaGraphCreate(&top, 0);
+  if (e != cudaSuccess) return e;
+  const int gz = occ_grid((const void*)k_dl_batch_init<WORDS>, threads, sms);
+  const int gi = occ_grid((const void*)k_dl_inspect<WORDS>, threads, sms);
+  const int gq = occ_grid((const void*)k_dl_qbuild, threads, sms);
+  const int gt = occ_grid((const void*)k_dl_td<WORDS>, threads, sms);
+  const int gu = occ_grid((const void*)k_dl_bu<WORDS>, threads, sms);
+  const int gd = occ_grid((const void*)k_dl_bu_defer<WORDS>, threads, sms);
+  const int go = occ_grid((const void*)k_dl_output<WORDS>, threads, sms);
+#define DL_TRY(call)                   \
+  do {                                 \
+    e = (call);                        \
+    if (e != cudaSuccess) {            \
+      cudaGraphDestroy(top);           \
+      return e;                        \
+    }                                  \
+  } while (0)
+  for (int g = 0; g < G; g++) {
+    CondH hb = 0, hl = 0, hd = 0;
+    DL_TRY(cudaGraphConditionalHandleCreate(&hb, top, 0, cudaGraphCondAssignDefault));
+    cudaGraphNode_t n0, n1;
+    DL_TRY(dl_kernel(top, &n0, nullptr, k_dl_start, 1, 32, p, g, hb, 0));
+    cudaGraph_t B = nullptr;
+    DL_TRY(dl_cond(top, &n1, n0, hb, cudaGraphCondTypeWhile, 1, &B));
+    DL_TRY(cudaGraphConditionalHandleCreate(&hl, B, 0, cudaGraphCondAssignDefault));
+    cudaGraphNode_t b0, b1, b2, b3, b4, b5;
+    DL_TRY(dl_kernel(B, &b0, nullptr, k_dl_batch_init<WORDS>, gz, threads, p, g, hl, 0));
+    DL_TRY(dl_kernel(B, &b1, b0, k_dl_seed<WORDS>, 1, 512, p, g, 0, 0));
+    DL_TRY(dl_kernel(B, &b2, b1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
+    cudaGraph_t L = nullptr;
+    DL_TRY(dl_cond(B, &b3, b2, hl, cudaGraphCondTypeWhile, 1, &L));
+    DL_TRY(dl_kernel(B, &b4, b3, k_dl_output<WORDS>, go, threads, p, g, 0, 0));
+    DL_TRY(dl_kernel(B, &b5, b4, k_dl_batch_end, 1, 32, p, g, hb, 0));
+    DL_TRY(cudaGraphConditionalHandleCreate(&hd, L, 2, cudaGraphCondAssignDefault));
+    cudaGraphNode_t l0, l1;
+    DL_TRY(dl_kernel(L, &l0, nullptr, k_dl_decide, 1, 32, p, g, hl, hd));
+    cudaGraph_t S[2] = {nullptr, nullptr};
+    DL_TRY(dl_cond(L, &l1, l0, hd, cudaGraphCondTypeSwitch, 2, S));
+    cudaGraphNode_t t0, t1, t2, u0, u1, u2;
+    DL_TRY(dl_kernel(S[0], &t0, nullptr, k_dl_qbuild, gq, threads, p, g, 0, 0));
+    DL_TRY(dl_kernel(S[0], &t1, t0, k_dl_td<WORDS>, gt, threads, p, g, 0, 0));
+    DL_TRY(dl_kernel(S[0], &t2, t1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
+    DL_TRY(dl_kernel(S[1], &u0, nullptr, k_dl_bu<WORDS>, gu, threads, p, g, 0, 0));
+    DL_TRY(dl_kernel(S[1], &u1, u0, k_dl_bu_defer<WORDS>, gd, threads, p, g, 0, 0));
+    DL_TRY(dl_kernel(S[1], &u2, u1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
+  }
+#undef DL_TRY
+  *out = top;
+  return cudaSuccess;
+}
 
 struct RunPlan {
   int words, C, nbatches, G, cpg, threads, grid, db;
@@ -549,7 +847,7 @@ extern "C" void ibfs_opts_default(ibfs_opts* o) {
   o->beta = 24.0f;
   o->sml_shed = 32;
   o->lrg_shed = 512;
-  o->mode = IBFS_MODE_PERSISTENT;
+  o->mode = IBFS_MODE_DEVICE_LOOP;
   o->groupby = 0;
   o->depth_bytes = 0;
   o->groups = 0;
@@ -635,6 +933,7 @@ static void destroy_graph(ibfs_graph* g) {
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
   g->gcache.release();
+  g->dlcache.release();
   for (auto& m : g->groups) m.release();
   g->beg.release();
   g->col.release();
@@ -843,6 +1142,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   rp.host_out = !(flags & IBFS_OUT_DEVICE);
   rp.smem = 0;
   const bool persistent = o.mode == IBFS_MODE_PERSISTENT;
+  const bool devloop = o.mode == IBFS_MODE_DEVICE_LOOP;
   // grid sizing
   int occ = 0;
   CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, persistent_for(rp.words, occ_level), rp.threads,
@@ -870,6 +1170,21 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     rp.G = G;
     rp.cpg = total_ctas / G;
     rp.grid = rp.cpg * G;
+  } else if (devloop) {
+    // concurrent batches are parallel branches of the graph; each kernel is
+    // sized by its own occupancy, so groups only overlap one batch's serial
+    // stretches (decisions, small levels) with another's work
+    int G = o.groups ? o.groups : 4;  // measured best on R-MAT scale 22-24
+    size_t freeb = 0, totb = 0;
+    if (G > 1 && cudaMemGetInfo(&freeb, &totb) == cudaSuccess) {
+      const size_t per = group_bytes(g->V, g->E, rp.words, rp.C, db, o.lrg_shed, rp.threads * 4,
+                                     false);
+      G = (int)std::max<size_t>(1, std::min<size_t>((size_t)G, (size_t)(freeb * 0.5) /
+                                                                  std::max<size_t>(per, 1)));
+    }
+    rp.G = std::max(1, std::min(G, rp.nbatches));
+    rp.cpg = total_ctas;
+    rp.grid = total_ctas;
   } else {
     rp.G = 1;
     rp.cpg = total_ctas;
@@ -888,11 +1203,12 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   ibfs_status bs;
   if ((bs = g->h_src.ensure(sizeof(int32_t) * n)) != IBFS_OK) return bs;
   if ((bs = g->h_outrow.ensure(sizeof(int32_t) * n)) != IBFS_OK) return bs;
-  if ((bs = g->d_src.ensure(sizeof(int32_t) * n)) != IBFS_OK) return bs;
-  if ((bs = g->d_outrow.ensure(sizeof(int32_t) * n)) != IBFS_OK) return bs;
-  if ((bs = g->d_brec.ensure(sizeof(BatchRec) * rp.nbatches)) != IBFS_OK) return bs;
+  if ((bs = g->d_src.ensure_pow2(sizeof(int32_t) * n)) != IBFS_OK) return bs;
+  if ((bs = g->d_outrow.ensure_pow2(sizeof(int32_t) * n)) != IBFS_OK) return bs;
+  if ((bs = g->d_brec.ensure_pow2(sizeof(BatchRec) * rp.nbatches)) != IBFS_OK) return bs;
   if ((bs = g->h_brec.ensure(sizeof(BatchRec) * rp.nbatches)) != IBFS_OK) return bs;
-  if ((bs = g->d_lrec.ensure(sizeof(LevelRec) * (size_t)rp.nbatches * kLrecCap)) != IBFS_OK) return bs;
+  if ((bs = g->d_lrec.ensure_pow2(sizeof(LevelRec) * (size_t)rp.nbatches * kLrecCap)) != IBFS_OK)
+    return bs;
   if ((bs = g->h_lrec.ensure(sizeof(LevelRec) * (size_t)rp.nbatches * kLrecCap)) != IBFS_OK) return bs;
   if ((bs = g->d_groups.ensure(sizeof(GroupBufs) * rp.G)) != IBFS_OK) return bs;
   if ((bs = g->h_par.ensure(sizeof(Ctl) * rp.G + sizeof(GroupBufs) * rp.G)) != IBFS_OK) return bs;
@@ -1041,6 +1357,54 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
       ibfs_status es2 = enqueue(s, false);
       if (es2 != IBFS_OK) return es2;
     }
+  } else if (devloop) {
+    // ---- device-driven schedule: one graph launch runs every level ------
+    CU(cudaMemcpyAsync(g->d_src.p, g->h_src.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(g->d_outrow.p, g->h_outrow.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(g->d_groups.p, hgb, sizeof(GroupBufs) * rp.G, cudaMemcpyHostToDevice, s));
+    Ctl* hctl = g->h_par.as<Ctl>();  // host staging of the G control blocks
+    for (int i = 0; i < rp.G; i++) {
+      std::memset(&hctl[i], 0, sizeof(Ctl));
+      hctl[i].ls.n_total = n;
+      hctl[i].ls.nbatches = rp.nbatches;
+      CU(cudaMemcpyAsync(hgb[i].ctl, &hctl[i], sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    }
+    CU(cudaMemsetAsync(g->d_brec.p, 0, sizeof(BatchRec) * rp.nbatches, s));
+    // the graph bakes in the launch Params (device pointers, graph sizes,
+    // options), the group count and the launch shapes: rebuild when any of
+    // them moves.  The run's source and batch counts travel in the control
+    // blocks instead, so runs of different sizes share one graph.
+    Params pk = p;
+    pk.n_total = 0;
+    pk.nbatches = 0;
+    std::string key(reinterpret_cast<const char*>(&pk), sizeof(pk));
+    const int shape[4] = {rp.G, rp.threads, g->sms, rp.words};
+    key.append(reinterpret_cast<const char*>(shape), sizeof(shape));
+    if (!(g->dlcache.exec && g->dlcache.key == key)) {
+      g->dlcache.release();
+      cudaGraph_t graph = nullptr;
+      cudaError_t be = DISPATCH_WORDS(rp.words, build_device_loop, p, rp.G, g->sms, rp.threads,
+                                      &graph);
+      if (be != cudaSuccess) {
+        last_cuda_error() = be;
+        (void)cudaGetLastError();
+        return IBFS_ERR_CUDA;
+      }
+      cudaGraphExec_t exec = nullptr;
+      cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) {
+        last_cuda_error() = ie;
+        (void)cudaGetLastError();
+        return IBFS_ERR_CUDA;
+      }
+      g->dlcache.exec = exec;
+      g->dlcache.key = key;
+    }
+    CU(cudaEventRecord(g->ev0, s));
+    CU(cudaGraphLaunch(g->dlcache.exec, s));
+    CU(cudaEventRecord(g->ev1, s));
+    if (rp.host_out) CU(cudaMemcpyAsync(depth_out, dout, out_bytes, cudaMemcpyDeviceToHost, s));
   } else {
     // ---- plain schedule -------------------------------------------------
     CU(cudaMemcpyAsync(g->d_src.p, g->h_src.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
@@ -1061,10 +1425,10 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
       CU(cudaMemsetAsync(gb.chg, 0, 2 * nchg * 4, s));
       CU(cudaMemsetAsync(gb.ctl, 0, sizeof(Ctl), s));
       CU(DISPATCH_WORDS(rp.words, launch_plain_seed, p, grid, thr, b, s));
-      CU(DISPATCH_WORDS(rp.words, launch_plain_inspect, p, gb, grid, thr, b, 0, 0, s));
+      CU(DISPATCH_WORDS(rp.words, launch_plain_inspect, p, gb, grid, thr, b, 0, s));
       launches += 2;
       int level = 0, cur_dir = kDirTD, max_level = 0, td = 0, bu = 0, err = 0;
-      unsigned long long m_u = (unsigned long long)g->E, teps = 0;
+      unsigned long long m_u = (unsigned long long)g->E, teps = 0, prev_changed = 0;
       while (true) {
         CU(cudaMemcpyAsync(hpar, &gb.ctl->par[level & 1], sizeof(Par), cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
@@ -1077,7 +1441,8 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
         else if (level + 1 > p.max_levels) { stop = 1; err = 3; }
         if (pr.changed && !pr.range_err) max_level = level;
         const int nd = choose_dir(level + 1, cur_dir, p.switch_level, p.alpha, p.beta, pr.changed,
-                                  pr.mf, m_u, p.V);
+                                  prev_changed, pr.mf, m_u, p.V);
+        prev_changed = pr.changed;
         if (level < kLrecCap) {
           LevelRec& r = hlr[(size_t)b * kLrecCap + level];
           r.batch = b; r.level = level; r.dir = level == 0 ? -1 : cur_dir; r.pad = 0;
@@ -1097,8 +1462,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
         CU(DISPATCH_WORDS(rp.words, launch_plain_level, p, gb, grid, thr, level, cur_dir, s));
         launches += 2;
         if (cur_dir == kDirTD) td++; else bu++;
-        CU(DISPATCH_WORDS(rp.words, launch_plain_inspect, p, gb, grid, thr, b, level,
-                          inspect_dense(pr.mf, p.V) ? 1 : 0, s));
+        CU(DISPATCH_WORDS(rp.words, launch_plain_inspect, p, gb, grid, thr, b, level, s));
         launches += 1;
       }
       BatchRec& r = hbr[b];
@@ -1115,7 +1479,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   }
   CU(cudaStreamSynchronize(s));
   // collect results
-  if (persistent) {
+  if (persistent || devloop) {
     CU(cudaMemcpy(g->h_brec.p, g->d_brec.p, sizeof(BatchRec) * rp.nbatches, cudaMemcpyDeviceToHost));
     CU(cudaMemcpy(g->h_lrec.p, g->d_lrec.p, sizeof(LevelRec) * (size_t)rp.nbatches * kLrecCap,
                   cudaMemcpyDeviceToHost));
@@ -1152,6 +1516,13 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
       st->bu_levels += br[b].bu;
       st->traversed_edges += (int64_t)br[b].teps;
     }
+    if (devloop) {
+      // kernel nodes that ran: start per group; per batch init, seed,
+      // inspect(0), output, end and one decide for the final level; per
+      // expanded level decide + two expand kernels + inspect
+      launches = rp.G;
+      for (int b = 0; b < rp.nbatches; b++) launches += 6 + 4LL * (br[b].td + br[b].bu);
+    }
     st->gpu_launches = launches;
     st->device_ms = ms;
     st->levels_len = 0;
@@ -1159,7 +1530,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
       const LevelRec* lr = g->h_lrec.as<LevelRec>();
       int k = 0;
       for (int b = 0; b < rp.nbatches && k < st->levels_cap; b++)
-        for (int l = 0; l <= std::min(br[b].levels + (persistent ? 1 : 0), kLrecCap - 1) &&
+        for (int l = 0; l <= std::min(br[b].levels + (persistent || devloop ? 1 : 0), kLrecCap - 1) &&
                         k < st->levels_cap; l++) {
           const LevelRec& r = lr[(size_t)b * kLrecCap + l];
           ibfs_level_rec& o2 = st->levels[k++];

@@ -52,7 +52,11 @@ typedef enum ibfs_mode {
        the reference's structure (bfs_gpu_opt.cuh:99-166) on sm_100a */
     IBFS_MODE_PLAIN = 0,
     /* one persistent level-synchronous launch for all levels of all batches */
-    IBFS_MODE_PERSISTENT = 1
+    IBFS_MODE_PERSISTENT = 1,
+    /* the PLAIN kernels (one per phase, each at its own occupancy) inside one
+       CUDA graph whose conditional nodes run the batch and level loops on
+       the device: no host round trip per level, no grid barrier */
+    IBFS_MODE_DEVICE_LOOP = 2
 } ibfs_mode;
 
 /* Layout of the depth output of ibfs_run. */
@@ -80,14 +84,16 @@ typedef struct ibfs_opts {
     float beta;            /* BU->TD when frontier_vertices < V/beta (24)         */
     int32_t sml_shed;      /* degree < sml_shed: one thread per vertex (default 32) */
     int32_t lrg_shed;      /* degree > lrg_shed: CTA chunks (default 512)         */
-    int32_t mode;          /* ibfs_mode                                           */
+    int32_t mode;          /* ibfs_mode (default IBFS_MODE_DEVICE_LOOP)           */
     int32_t groupby;       /* 1: reorder sources with GroupBy before batching     */
     int32_t depth_bytes;   /* 1 (INFTY 255) or 2 (INFTY 65535); 0: 1, widened to 2
                               automatically when a level exceeds 254              */
-    int32_t groups;        /* batches run concurrently in one launch (0: auto)    */
+    int32_t groups;        /* batches run concurrently (0: auto; device loop: 4)  */
     int32_t threads;       /* threads per CTA (0: 512)                            */
     int32_t ctas_per_sm;   /* persistent grid = SMs * ctas_per_sm (0: auto)       */
-    int32_t use_graph;     /* 1: capture the run in a CUDA graph, replay on reuse */
+    int32_t use_graph;     /* persistent: 1 captures the run in a CUDA graph and
+                              replays it on reuse (the device loop is always a
+                              graph, rebuilt only when buffers or options move)   */
     int32_t timeout_ms;    /* budget of every bounded device wait (0: 10000)      */
     int32_t max_levels;    /* abort with IBFS_ERR_RANGE beyond this (0: 65534)    */
     int32_t debug_withhold;/* test hook: CTA 0 never arrives at its first grid
@@ -105,12 +111,14 @@ typedef struct ibfs_opts {
 typedef struct ibfs_level_rec {
     int32_t batch;         /* batch index                                         */
     int32_t level;         /* level expanded                                      */
-    int32_t dir;           /* 0 top-down, 1 bottom-up                             */
+    int32_t dir;           /* 0 top-down, 1 bottom-up, -1 level 0 (seeding),
+                              2 the batch's output pass (persistent, device loop) */
     int32_t pad;
     int64_t frontier;      /* vertices whose status changed at this level         */
     int64_t frontier_edges;/* sum of their degrees                                */
     int64_t expand_ns;     /* device time of the level's expand phase (persistent
-                              schedule; 0 otherwise; level 0: seeding)            */
+                              and device loop; 0 in the plain schedule; level 0:
+                              seeding; dir 2: the output pass)                    */
     int64_t inspect_ns;    /* device time of its inspect phase                    */
 } ibfs_level_rec;
 
@@ -231,8 +239,9 @@ ibfs_status ibfs_server_destroy(ibfs_server *s);
 
 /* Per-graph tuning (no counterpart in the reference, whose constants are
    fixed at comm.h:25-30 and ibfs.cu:71-72): coordinate descent over width,
-   alpha/beta, queue thresholds, CTA size and concurrent batches, each trial
-   a real persistent run of `src` (device output, `reps` timed repeats).
+   alpha/beta, queue thresholds, occupancy (persistent schedule) and
+   concurrent batches, each trial a real run of `src` in the base options'
+   schedule (device output, `reps` timed repeats).
    `best` receives the winner; `log` (optional) one JSON object per trial. */
 ibfs_status ibfs_autotune(ibfs_graph *g, const int32_t *src_host, int64_t n,
                           const ibfs_opts *base, int32_t reps, ibfs_opts *best,

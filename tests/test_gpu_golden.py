@@ -18,7 +18,7 @@ def test_gpu_depths_match_golden(path, width):
     f = dict(np.load(path))
     g = ib.Graph.from_csr(f["beg"], f["col"])
     try:
-        for mode in (ib.MODE_PLAIN, ib.MODE_PERSISTENT):
+        for mode in (ib.MODE_PLAIN, ib.MODE_PERSISTENT, ib.MODE_DEVICE_LOOP):
             res = g.run(f["src"], width=width, mode=mode, groupby=1)
             assert np.array_equal(res.depth, f["depth"])
             assert res.stats["traversed_edges"] == int(f["ref_report"][:, 1].sum())

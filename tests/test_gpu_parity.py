@@ -1,7 +1,7 @@
 """GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
 
 Integer work, so the bar is bit-exact depths for every source and an exact
-traversed-edge count.  Covers every status width, both schedules, both output
+traversed-edge count.  Covers every status width, all three schedules, both output
 layouts, partial and multiple batches, several concurrent groups, GroupBy,
 the fixed and the alpha/beta direction switch, one- and two-byte depths, and
 the edge cases of the reference's inputs (isolated and duplicated sources,
@@ -16,6 +16,7 @@ import oracle
 pytestmark = pytest.mark.gpu
 
 WIDTHS = [32, 64, 128, 256]
+MODES = [ib.MODE_PLAIN, ib.MODE_PERSISTENT, ib.MODE_DEVICE_LOOP]
 
 
 def _graph(kind: str):
@@ -68,7 +69,7 @@ def run_and_check(beg, col, g, src, layout=ib.LAYOUT_SOURCE_MAJOR, **kw):
 
 
 @pytest.mark.parametrize("width", WIDTHS)
-@pytest.mark.parametrize("mode", [ib.MODE_PLAIN, ib.MODE_PERSISTENT])
+@pytest.mark.parametrize("mode", MODES)
 def test_rmat_widths_modes(width, mode):
     beg, col, g = graph("rmat13")
     src = ib.sample_sources(beg, col, width, seed=1)
@@ -76,22 +77,24 @@ def test_rmat_widths_modes(width, mode):
 
 
 @pytest.mark.parametrize("width", WIDTHS)
-def test_partial_and_multi_batch(width):
+@pytest.mark.parametrize("mode", [ib.MODE_PERSISTENT, ib.MODE_DEVICE_LOOP])
+def test_partial_and_multi_batch(width, mode):
     beg, col, g = graph("rmat10")
     src = ib.sample_sources(beg, col, 2 * width + 7, seed=3)
-    run_and_check(beg, col, g, src, width=width, mode=ib.MODE_PERSISTENT)
-    run_and_check(beg, col, g, src[:5], width=width, mode=ib.MODE_PERSISTENT)
+    run_and_check(beg, col, g, src, width=width, mode=mode)
+    run_and_check(beg, col, g, src[:5], width=width, mode=mode)
 
 
 @pytest.mark.parametrize("groups", [1, 2, 3, 5])
-def test_groups(groups):
+@pytest.mark.parametrize("mode", [ib.MODE_PERSISTENT, ib.MODE_DEVICE_LOOP])
+def test_groups(groups, mode):
     beg, col, g = graph("rmat13")
     src = ib.sample_sources(beg, col, 5 * 64, seed=7)
-    run_and_check(beg, col, g, src, width=64, mode=ib.MODE_PERSISTENT, groups=groups)
+    run_and_check(beg, col, g, src, width=64, mode=mode, groups=groups)
 
 
 @pytest.mark.parametrize("layout", [ib.LAYOUT_SOURCE_MAJOR, ib.LAYOUT_VERTEX_MAJOR])
-@pytest.mark.parametrize("mode", [ib.MODE_PLAIN, ib.MODE_PERSISTENT])
+@pytest.mark.parametrize("mode", MODES)
 def test_layouts(layout, mode):
     beg, col, g = graph("rmat10")
     src = ib.sample_sources(beg, col, 300, seed=5)
@@ -105,13 +108,15 @@ def test_graph_families(kind):
     src = ib.sample_sources(beg, col, 256, seed=9)
     run_and_check(beg, col, g, src, width=128, mode=ib.MODE_PERSISTENT)
     run_and_check(beg, col, g, src[:128], width=256, mode=ib.MODE_PLAIN)
+    run_and_check(beg, col, g, src, width=64, mode=ib.MODE_DEVICE_LOOP, groups=2)
 
 
 @pytest.mark.parametrize("sw", [0, 1, 2, 5, 1000])
-def test_fixed_switch_level(sw):
+@pytest.mark.parametrize("mode", [ib.MODE_PERSISTENT, ib.MODE_DEVICE_LOOP])
+def test_fixed_switch_level(sw, mode):
     beg, col, g = graph("rmat13")
     src = ib.sample_sources(beg, col, 128, seed=2)
-    res = run_and_check(beg, col, g, src, width=128, switch_level=sw, levels_cap=64)
+    res = run_and_check(beg, col, g, src, width=128, switch_level=sw, levels_cap=64, mode=mode)
     dirs = [r["dir"] for r in res.levels if r["level"] > 0 and r["dir"] != 2]
     for r in res.levels:
         if r["level"] > 0 and r["dir"] != 2:  # dir 2: the batch's output pass
@@ -145,7 +150,7 @@ def test_edge_case_graph():
     g = ib.Graph.from_csr(beg, col)
     src = np.array([0, 40, 4, 7, 7, 39, 2, 0], np.int32)  # isolated + duplicates
     for w in WIDTHS:
-        for mode in (ib.MODE_PLAIN, ib.MODE_PERSISTENT):
+        for mode in MODES:
             run_and_check(beg, col, g, src, width=w, mode=mode)
     g.close()
 
@@ -156,7 +161,7 @@ def test_long_path_uint16_widening():
     beg, col = ib.csr_from_edges(u, u + 1, n)
     g = ib.Graph.from_csr(beg, col)
     src = np.array([0, n - 1, n // 2], np.int32)
-    for mode in (ib.MODE_PLAIN, ib.MODE_PERSISTENT):
+    for mode in MODES:
         res = run_and_check(beg, col, g, src, width=32, mode=mode)
         assert res.depth.dtype == np.uint16
         assert res.stats["max_level"] == n - 1
@@ -179,7 +184,8 @@ def test_graph_replay_and_stream():
     try:
         for it in range(3):
             out.fill_(7)
-            res = g.run(src, width=128, use_graph=1, on_device=True, out_ptr=out.data_ptr())
+            res = g.run(src, width=128, use_graph=1, mode=ib.MODE_PERSISTENT, on_device=True,
+                        out_ptr=out.data_ptr())
             s.synchronize()
             assert np.array_equal(out.cpu().numpy(), ref)
             if it > 0:
@@ -221,3 +227,29 @@ def test_bytes_alg_matches_oracle():
     dev = torch.from_numpy(ref).cuda()
     for w in (64, 128):
         assert g.bytes_alg(dev.data_ptr(), len(src), 1, w) == oracle.bytes_alg(beg, col, ref, w)
+
+
+def test_device_loop_replay_and_records():
+    """The device-driven graph is built once and replayed; its level records
+    carry the same frontiers as the persistent kernel's."""
+    import torch
+
+    beg, col, g = graph("rmat13")
+    src = ib.sample_sources(beg, col, 256, seed=14)
+    ref, _ = oracle.bfs(beg, col, src)
+    out = torch.empty((len(src), len(beg) - 1), dtype=torch.uint8, device="cuda")
+    recs = {}
+    for mode in (ib.MODE_PERSISTENT, ib.MODE_DEVICE_LOOP):
+        for it in range(2):
+            out.fill_(7)
+            res = g.run(src, width=128, mode=mode, on_device=True, out_ptr=out.data_ptr(),
+                        levels_cap=256)
+            torch.cuda.synchronize()
+            assert np.array_equal(out.cpu().numpy(), ref)
+        recs[mode] = [(r["batch"], r["level"], r["dir"], r["frontier"], r["frontier_edges"])
+                      for r in res.levels]
+        if mode == ib.MODE_DEVICE_LOOP:
+            st = res.stats
+            assert st["gpu_launches"] == (st["groups"] + 6 * st["n_batches"]
+                                          + 4 * (st["td_levels"] + st["bu_levels"]))
+    assert recs[ib.MODE_PERSISTENT] == recs[ib.MODE_DEVICE_LOOP]
