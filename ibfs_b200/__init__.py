@@ -6,6 +6,7 @@ sm_100a kernels; this package is its Python binding and build helper.
 from .api import (  # noqa: F401
     LAYOUT_SOURCE_MAJOR,
     LAYOUT_VERTEX_MAJOR,
+    MODE_AUTO,
     MODE_DEVICE_LOOP,
     MODE_PERSISTENT,
     MODE_PLAIN,

@@ -22,7 +22,7 @@ STATUS_NAMES = {
     0: "OK", 1: "IO", 2: "FORMAT", 3: "RANGE", 4: "OOM", 5: "CUDA", 6: "TIMEOUT",
     7: "INVALID_ARG", 8: "UNSUPPORTED", 9: "BUSY", 10: "NOT_FOUND",
 }
-MODE_PLAIN, MODE_PERSISTENT, MODE_DEVICE_LOOP = 0, 1, 2
+MODE_PLAIN, MODE_PERSISTENT, MODE_DEVICE_LOOP, MODE_AUTO = 0, 1, 2, 3
 LAYOUT_SOURCE_MAJOR, LAYOUT_VERTEX_MAJOR = 0, 1
 OUT_DEVICE = 1
 

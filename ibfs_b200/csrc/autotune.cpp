@@ -54,13 +54,15 @@ extern "C" ibfs_status ibfs_autotune(ibfs_graph* g, const int32_t* src, int64_t 
   ibfs_opts o0;
   if (base) o0 = *base;
   else ibfs_opts_default(&o0);
-  if (o0.mode == IBFS_MODE_PLAIN) o0.mode = IBFS_MODE_DEVICE_LOOP;  // no host loop in trials
+  int64_t V = 0, E = 0;
+  ibfs_graph_info(g, &V, &E, nullptr);
+  if (o0.mode == IBFS_MODE_PLAIN || o0.mode == IBFS_MODE_AUTO)  // fix the schedule for all trials
+    o0.mode = (double)V * (o0.width / 8) <= 32.0 * 1024 * 1024 ? IBFS_MODE_PERSISTENT
+                                                                 : IBFS_MODE_DEVICE_LOOP;
   const bool persistent = o0.mode == IBFS_MODE_PERSISTENT;
   o0.use_graph = 1;
   if (o0.depth_bytes == 0) o0.depth_bytes = 1;
   if (reps < 1) reps = 2;
-  int64_t V = 0, E = 0;
-  ibfs_graph_info(g, &V, &E, nullptr);
   void* dout = nullptr;
   if (cudaMalloc(&dout, (size_t)n * (size_t)V * o0.depth_bytes) != cudaSuccess) {
     (void)cudaGetLastError();

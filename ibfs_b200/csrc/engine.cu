@@ -573,7 +573,7 @@ static ibfs_status check_opts(const ibfs_opts* o) {
     return IBFS_ERR_INVALID_ARG;
   if (o->concurrent < 0 || o->concurrent > o->width) return IBFS_ERR_INVALID_ARG;
   if (o->mode != IBFS_MODE_PLAIN && o->mode != IBFS_MODE_PERSISTENT &&
-      o->mode != IBFS_MODE_DEVICE_LOOP)
+      o->mode != IBFS_MODE_DEVICE_LOOP && o->mode != IBFS_MODE_AUTO)
     return IBFS_ERR_INVALID_ARG;
   if (o->depth_bytes != 0 && o->depth_bytes != 1 && o->depth_bytes != 2) return IBFS_ERR_INVALID_ARG;
   if (o->threads != 0 && o->threads != 128 && o->threads != 256 && o->threads != 512)
@@ -847,7 +847,7 @@ extern "C" void ibfs_opts_default(ibfs_opts* o) {
   o->beta = 24.0f;
   o->sml_shed = 32;
   o->lrg_shed = 512;
-  o->mode = IBFS_MODE_DEVICE_LOOP;
+  o->mode = IBFS_MODE_AUTO;
   o->groupby = 0;
   o->depth_bytes = 0;
   o->groups = 0;
@@ -1125,10 +1125,25 @@ extern "C" ibfs_status ibfs_run(ibfs_graph* g, const int32_t* src_host, int64_t 
   return s;
 }
 
-static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const ibfs_opts& o,
+// IBFS_MODE_AUTO: small graphs (one batch's status words within 32 MB, a
+// few levels of short kernels) run the persistent kernel from a CUDA graph,
+// where the device loop's per-kernel launch costs would dominate; larger
+// ones run the device loop.
+static ibfs_opts resolve_mode(const ibfs_graph* g, const ibfs_opts& in) {
+  ibfs_opts o = in;
+  if (o.mode == IBFS_MODE_AUTO) {
+    const bool small = (double)g->V * (o.width / 8) <= 32.0 * 1024 * 1024;
+    o.mode = small ? IBFS_MODE_PERSISTENT : IBFS_MODE_DEVICE_LOOP;
+    if (small && !o.debug_withhold) o.use_graph = 1;
+  }
+  return o;
+}
+
+static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const ibfs_opts& o_in,
                             int db, void* depth_out, int32_t layout, uint32_t flags,
                             ibfs_stats* st, bool* range_hit, const int32_t* rows_in) {
   *range_hit = false;
+  const ibfs_opts o = resolve_mode(g, o_in);
   cudaStream_t s = g->stream;
   RunPlan rp;
   std::memset(&rp, 0, sizeof(rp));
@@ -1157,9 +1172,9 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
       const int64_t want = std::max<int64_t>(1, (g->V + 32LL * 8 * (rp.threads / 32) - 1) /
                                                     (32LL * 8 * (rp.threads / 32)));
       G = (int)std::max<int64_t>(1, std::min<int64_t>(rp.nbatches, total_ctas / std::min<int64_t>(want, total_ctas)));
-      // memory guard
+      // memory guard (only when the workspace has to grow to G groups)
       size_t freeb = 0, totb = 0;
-      if (cudaMemGetInfo(&freeb, &totb) == cudaSuccess) {
+      if ((int)g->groups.size() < G && cudaMemGetInfo(&freeb, &totb) == cudaSuccess) {
         const size_t per = group_bytes(g->V, g->E, rp.words, rp.C, db, o.lrg_shed, rp.threads * 4,
                                        false);
         const size_t budget = (size_t)(freeb * 0.5);
@@ -1174,9 +1189,9 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     // concurrent batches are parallel branches of the graph; each kernel is
     // sized by its own occupancy, so groups only overlap one batch's serial
     // stretches (decisions, small levels) with another's work
-    int G = o.groups ? o.groups : 4;  // measured best on R-MAT scale 22-24
+    int G = std::min(o.groups ? o.groups : 4, rp.nbatches);  // 4: best on R-MAT s22-24
     size_t freeb = 0, totb = 0;
-    if (G > 1 && cudaMemGetInfo(&freeb, &totb) == cudaSuccess) {
+    if (G > 1 && (int)g->groups.size() < G && cudaMemGetInfo(&freeb, &totb) == cudaSuccess) {
       const size_t per = group_bytes(g->V, g->E, rp.words, rp.C, db, o.lrg_shed, rp.threads * 4,
                                      false);
       G = (int)std::max<size_t>(1, std::min<size_t>((size_t)G, (size_t)(freeb * 0.5) /
@@ -1480,15 +1495,18 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   CU(cudaStreamSynchronize(s));
   // collect results
   if (persistent || devloop) {
-    CU(cudaMemcpy(g->h_brec.p, g->d_brec.p, sizeof(BatchRec) * rp.nbatches, cudaMemcpyDeviceToHost));
-    CU(cudaMemcpy(g->h_lrec.p, g->d_lrec.p, sizeof(LevelRec) * (size_t)rp.nbatches * kLrecCap,
-                  cudaMemcpyDeviceToHost));
+    CU(cudaMemcpyAsync(g->h_brec.p, g->d_brec.p, sizeof(BatchRec) * rp.nbatches,
+                       cudaMemcpyDeviceToHost, s));
+    if (st && st->levels && st->levels_cap > 0)
+      CU(cudaMemcpyAsync(g->h_lrec.p, g->d_lrec.p, sizeof(LevelRec) * (size_t)rp.nbatches * kLrecCap,
+                         cudaMemcpyDeviceToHost, s));
+    int* herr = reinterpret_cast<int*>(g->h_par.p);  // the staged control blocks are done with
+    for (int i = 0; i < rp.G; i++)
+      CU(cudaMemcpyAsync(&herr[i], &hgb[i].ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
     int gerr = 0;
-    for (int i = 0; i < rp.G; i++) {
-      int e = 0;
-      CU(cudaMemcpy(&e, &hgb[i].ctl->err, sizeof(int), cudaMemcpyDeviceToHost));
-      if (e && !gerr) gerr = e;
-    }
+    for (int i = 0; i < rp.G; i++)
+      if (herr[i] && !gerr) gerr = herr[i];
     if (gerr) {
       *range_hit = gerr == 3;
       return (ibfs_status)gerr;

@@ -197,7 +197,7 @@ static void worker_loop(ibfs_server* s) {
     std::memset(&rs, 0, sizeof(rs));
     ibfs_opts ro = s->so.run;
     ro.depth_bytes = s->db;
-    ro.mode = IBFS_MODE_DEVICE_LOOP;
+    if (ro.mode == IBFS_MODE_PLAIN) ro.mode = IBFS_MODE_AUTO;  // no host level loop here
     ro.use_graph = 0;
     ro.groupby = 0;
     const ibfs_status rc = run_rows(s->g, ord.data(), ordrows.data(), n, ro, s->arena, &rs);

@@ -56,7 +56,11 @@ typedef enum ibfs_mode {
     /* the PLAIN kernels (one per phase, each at its own occupancy) inside one
        CUDA graph whose conditional nodes run the batch and level loops on
        the device: no host round trip per level, no grid barrier */
-    IBFS_MODE_DEVICE_LOOP = 2
+    IBFS_MODE_DEVICE_LOOP = 2,
+    /* the default: PERSISTENT (with use_graph) when one batch's status words
+       fit in 32 MB, where per-kernel launch costs would dominate; DEVICE_LOOP
+       above that */
+    IBFS_MODE_AUTO = 3
 } ibfs_mode;
 
 /* Layout of the depth output of ibfs_run. */
@@ -84,7 +88,7 @@ typedef struct ibfs_opts {
     float beta;            /* BU->TD when frontier_vertices < V/beta (24)         */
     int32_t sml_shed;      /* degree < sml_shed: one thread per vertex (default 32) */
     int32_t lrg_shed;      /* degree > lrg_shed: CTA chunks (default 512)         */
-    int32_t mode;          /* ibfs_mode (default IBFS_MODE_DEVICE_LOOP)           */
+    int32_t mode;          /* ibfs_mode (default IBFS_MODE_AUTO)                  */
     int32_t groupby;       /* 1: reorder sources with GroupBy before batching     */
     int32_t depth_bytes;   /* 1 (INFTY 255) or 2 (INFTY 65535); 0: 1, widened to 2
                               automatically when a level exceeds 254              */
