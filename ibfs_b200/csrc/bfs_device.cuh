@@ -129,7 +129,8 @@ struct Params {
   LevelRec* lrec;
   int lrec_cap;
   int vec_out;  // vertex-major rows allow 4-byte stores (n_b*db % 4 == 0, aligned base)
-  int vec_sm;   // source-major rows allow 4-vertex stores (V % 4 == 0, aligned base)
+  int vec_sm;   // source-major rows allow vector stores of this many bytes: 16 (V % 16
+                // == 0, 16-byte aligned base), 4 (V % 4 == 0, 4-byte aligned) or 0
   int bu_filter;    // bottom-up skips neighbours outside the previous frontier
   int col_vec;      // col is 16-byte aligned and padded by 4 entries (vector reads)
   int hub_t;        // bottom-up: a warp scans at most hub_t neighbours of a vertex;
@@ -906,26 +907,39 @@ __device__ __forceinline__ void interleave4(const uint32_t (&x)[4], uint32_t (&y
 }
 
 // Source-major, one-byte depths, NP planes known at compile time: lane =
-// 4 consecutive vertices, one 4-byte store per source.
-template <int WORDS, int NP>
+// VPL consecutive vertices (groups of 4 interleaved at a time), one VPL-byte
+// store per source row, so a warp writes 32*VPL contiguous bytes of a row
+// per store instruction.  4 measured best on B200 (R-MAT scale 24: output
+// pass 1.20 ms per batch at 4, 1.62 at 8, 1.79 at 16): the wider lanes need
+// more registers than the extra store width saves.
+#ifndef IBFS_OUT_VPL
+#define IBFS_OUT_VPL 4
+#endif
+template <int WORDS, int NP, int VPL>
 __device__ void output_sm_u8(const Params& p, const GroupBufs& gb, const int32_t* rows, int n_b,
                              const Team& t) {
+  constexpr int NG = VPL / 4;
   const int lane = t.lane;
-  for (long long base = t.warp * 128; base < p.V; base += t.nwarps * 128) {
-    const long long v0 = base + 4 * lane;
-    const bool full4 = p.vec_sm && v0 + 3 < p.V;
+  for (long long base = t.warp * (32LL * VPL); base < p.V; base += t.nwarps * (32LL * VPL)) {
+    const long long v0 = base + (long long)VPL * lane;
+    const bool fullv = p.vec_sm >= VPL && v0 + VPL - 1 < p.V;
 #pragma unroll 1
     for (int k = 0; k < WORDS && k * 32 < n_b; k++) {
-      uint32_t x[4], ys[4], yp[NP > 0 ? NP : 1][4];
+      uint32_t ys[NG][4], yp[NP > 0 ? NP : 1][NG][4];
 #pragma unroll
-      for (int i = 0; i < 4; i++) x[i] = v0 + i < p.V ? gb.last[(size_t)(v0 + i) * WORDS + k] : 0u;
-      interleave4(x, ys);
+      for (int g = 0; g < NG; g++) {
+        uint32_t x[4];
+        const long long vg = v0 + 4 * g;
 #pragma unroll
-      for (int b = 0; b < NP; b++) {
-        const uint32_t* pl = gb.planes + (size_t)b * p.plane_stride;
+        for (int i = 0; i < 4; i++) x[i] = vg + i < p.V ? gb.last[(size_t)(vg + i) * WORDS + k] : 0u;
+        interleave4(x, ys[g]);
 #pragma unroll
-        for (int i = 0; i < 4; i++) x[i] = v0 + i < p.V ? pl[(size_t)(v0 + i) * WORDS + k] : 0u;
-        interleave4(x, yp[b]);
+        for (int b = 0; b < NP; b++) {
+          const uint32_t* pl = gb.planes + (size_t)b * p.plane_stride;
+#pragma unroll
+          for (int i = 0; i < 4; i++) x[i] = vg + i < p.V ? pl[(size_t)(vg + i) * WORDS + k] : 0u;
+          interleave4(x, yp[b][g]);
+        }
       }
       const int js = min(32, n_b - k * 32);
 #pragma unroll
@@ -934,15 +948,27 @@ __device__ void output_sm_u8(const Params& p, const GroupBufs& gb, const int32_t
         for (int r = 0; r < 8; r++) {
           const int j = q * 8 + r;
           if (j < js) {
-            uint32_t w = nib_to_bytes(~(ys[q] >> (4 * r)) & 0xFu) * 0xFFu;
+            uint32_t w[NG];
 #pragma unroll
-            for (int b = 0; b < NP; b++) w |= nib_to_bytes((yp[b][q] >> (4 * r)) & 0xFu) << b;
+            for (int g = 0; g < NG; g++) {
+              w[g] = nib_to_bytes(~(ys[g][q] >> (4 * r)) & 0xFu) * 0xFFu;
+#pragma unroll
+              for (int b = 0; b < NP; b++) w[g] |= nib_to_bytes((yp[b][g][q] >> (4 * r)) & 0xFu) << b;
+            }
             uint8_t* row = p.out + (size_t)rows[k * 32 + j] * (size_t)p.V;
-            if (full4) {
-              *reinterpret_cast<uint32_t*>(row + v0) = w;
+            if (fullv) {
+              if constexpr (VPL == 16) {
+                *reinterpret_cast<uint4*>(row + v0) = make_uint4(w[0], w[1], w[2], w[3]);
+              } else if constexpr (VPL == 8) {
+                *reinterpret_cast<uint2*>(row + v0) = make_uint2(w[0], w[1]);
+              } else {
+                *reinterpret_cast<uint32_t*>(row + v0) = w[0];
+              }
             } else {
-              for (int i = 0; i < 4; i++)
-                if (v0 + i < p.V) row[v0 + i] = (uint8_t)(w >> (8 * i));
+#pragma unroll
+              for (int g = 0; g < NG; g++)
+                for (int i = 0; i < 4; i++)
+                  if (v0 + 4 * g + i < p.V) row[v0 + 4 * g + i] = (uint8_t)(w[g] >> (8 * i));
             }
           }
         }
@@ -1009,24 +1035,31 @@ __device__ void output_generic(const Params& p, const GroupBufs& gb, uint8_t* de
   }
 }
 
-template <int WORDS, int NP>
+// VPL: vertices per lane of the source-major path when the rows allow
+// vector stores of that width (the persistent kernel, at 64 registers,
+// keeps 4).
+template <int WORDS, int NP, int VPL>
 __device__ __forceinline__ void output_u8(const Params& p, const GroupBufs& gb, uint8_t* depth_vm,
                                           const int32_t* rows, int n_b, const Team& t) {
-  if (p.layout == 0) output_sm_u8<WORDS, NP>(p, gb, rows, n_b, t);
-  else output_vm_u8<WORDS, NP>(p, gb, depth_vm, n_b, t);
+  if (p.layout == 0) {
+    if (p.vec_sm >= VPL) output_sm_u8<WORDS, NP, VPL>(p, gb, rows, n_b, t);
+    else output_sm_u8<WORDS, NP, 4>(p, gb, rows, n_b, t);
+  } else {
+    output_vm_u8<WORDS, NP>(p, gb, depth_vm, n_b, t);
+  }
 }
 
-template <int WORDS>
+template <int WORDS, int VPL = IBFS_OUT_VPL>
 __device__ void output_phase(const Params& p, const GroupBufs& gb, uint8_t* depth_vm,
                              const int32_t* rows, int n_b, int max_level, const Team& t) {
   const int P = planes_for(max_level);
   if (p.db == 1) {
     switch (P) {
-      case 0: output_u8<WORDS, 0>(p, gb, depth_vm, rows, n_b, t); return;
-      case 1: output_u8<WORDS, 1>(p, gb, depth_vm, rows, n_b, t); return;
-      case 2: output_u8<WORDS, 2>(p, gb, depth_vm, rows, n_b, t); return;
-      case 3: output_u8<WORDS, 3>(p, gb, depth_vm, rows, n_b, t); return;
-      case 4: output_u8<WORDS, 4>(p, gb, depth_vm, rows, n_b, t); return;
+      case 0: output_u8<WORDS, 0, VPL>(p, gb, depth_vm, rows, n_b, t); return;
+      case 1: output_u8<WORDS, 1, VPL>(p, gb, depth_vm, rows, n_b, t); return;
+      case 2: output_u8<WORDS, 2, VPL>(p, gb, depth_vm, rows, n_b, t); return;
+      case 3: output_u8<WORDS, 3, VPL>(p, gb, depth_vm, rows, n_b, t); return;
+      case 4: output_u8<WORDS, 4, VPL>(p, gb, depth_vm, rows, n_b, t); return;
       default: break;
     }
   }

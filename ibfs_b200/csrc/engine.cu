@@ -1,15 +1,18 @@
-// engine.cu -- kernels, the resident-graph handle and the ibfs_run schedules.
+// engine.cu -- the resident-graph handle, ibfs_run and two of its schedules.
 //
-// Two schedules over the same phase functions (bfs_device.cuh):
-//   PLAIN       host-driven level loop: one launch per phase and a host
-//               synchronisation per level to read the counters -- the shape
-//               of the reference's ibfs() loop (bfs_gpu_opt.cuh:99-166);
-//   PERSISTENT  one cooperative launch runs every level of every batch: the
-//               grid is cut into G groups of CTAs, each group owns one batch
-//               at a time and synchronises with a bounded team barrier; the
-//               direction decision is taken on the device.  Optionally the
-//               whole run (uploads, launch, downloads) is captured once in a
-//               CUDA graph and replayed.
+// Three schedules run the same phase functions (bfs_device.cuh):
+//   PLAIN        host-driven level loop: one launch per phase and a host
+//                synchronisation per level to read the counters -- the shape
+//                of the reference's ibfs() loop (bfs_gpu_opt.cuh:99-166);
+//   PERSISTENT   one cooperative launch runs every level of every batch: the
+//                grid is cut into G groups of CTAs, each group owns one batch
+//                at a time and synchronises with a bounded team barrier; the
+//                direction decision is taken on the device.  Optionally the
+//                whole run (uploads, launch, downloads) is captured once in a
+//                CUDA graph and replayed;
+//   DEVICE_LOOP  the plain kernels inside one CUDA graph whose conditional
+//                nodes run the batch and level loops (devloop.cu).
+// AUTO picks PERSISTENT for small graphs and DEVICE_LOOP otherwise.
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -24,37 +27,13 @@
 
 #include "bfs_device.cuh"
 #include "internal.h"
+#include "launch_common.cuh"
 
 namespace ibfs {
 
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ Team make_team(int block, int nblocks) {
-  Team t;
-  t.block = block;
-  t.nblocks = nblocks;
-  t.tid = (long long)block * blockDim.x + threadIdx.x;
-  t.nthreads = (long long)nblocks * blockDim.x;
-  t.warp = t.tid >> 5;
-  t.nwarps = t.nthreads >> 5;
-  t.lane = threadIdx.x & 31;
-  return t;
-}
-
-__device__ __forceinline__ int depth_limit(int db) { return db == 1 ? 254 : 65534; }
-
-__device__ __forceinline__ uint8_t* batch_depth(const Params& p, int b) {
-  return p.layout == 1 ? p.out + (size_t)b * (size_t)p.V * p.C * p.db : nullptr;
-}
-
-// Output rows of batch b (source-major) into shared memory.
-__device__ __forceinline__ void load_rows(const Params& p, int b, int n_b, int32_t* s_rows) {
-  if (p.layout == 0)
-    for (int j = threadIdx.x; j < n_b; j += blockDim.x) s_rows[j] = p.out_row[(long long)b * p.C + j];
-  __syncthreads();
-}
-
 // THREADS x MINB fixes the register budget (65536 / (THREADS * MINB)) and
 // hence how many warps per SM hide the latency of the random gathers.
 template <int WORDS, int THREADS, int MINB>
@@ -175,7 +154,7 @@ __global__ void __launch_bounds__(THREADS, MINB) persistent_kernel(Params p) {
       }
       return;
     }
-    output_phase<WORDS>(p, gb, batch_depth(p, b), s_rows, n_b, s_maxl, t);
+    output_phase<WORDS, 4>(p, gb, batch_depth(p, b), s_rows, n_b, s_maxl, t);
     if (lead && level + 1 < p.lrec_cap) {
       // one extra record per batch: dir 2 = the output pass
       LevelRec r;
@@ -252,200 +231,6 @@ __global__ void __launch_bounds__(512) k_output(Params p, GroupBufs gb, int b, i
   const int n_b = (int)min((long long)p.C, p.n_total - k0);
   load_rows(p, b, n_b, s_rows);
   output_phase<WORDS>(p, gb, batch_depth(p, b), s_rows, n_b, max_level, t);
-}
-
-// ---- device-driven schedule ------------------------------------------------
-// The plain schedule's kernels inside one CUDA graph whose conditional nodes
-// run the batch loop (WHILE) and the level loop (WHILE, with a SWITCH on the
-// direction), so that every phase keeps the register budget and occupancy of
-// its own kernel while no level needs a host round trip.  The batch and the
-// level come from the group's LoopState; the decision kernel is the
-// persistent kernel's top-of-level block (same rule, same records) run by one
-// thread.  All kernels share one signature so that the graph builder can
-// bind them uniformly: (params, group, handle 0, handle 1).
-using CondH = cudaGraphConditionalHandle;
-
-// The run's source and batch counts come from the control block, not from
-// Params, so that one built graph serves runs of any size.
-__device__ __forceinline__ int dl_batch_size(const Params& p, const LoopState& ls, int b) {
-  return (int)min((long long)p.C, ls.n_total - (long long)b * p.C);
-}
-
-// First batch of group g; the batch loop runs while it exists.
-__global__ void k_dl_start(Params p, int g, CondH h_batch, CondH) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  Ctl* ctl = p.groups[g].ctl;
-  ctl->ls.batch = g;
-  ctl->ls.err = 0;
-  cudaGraphSetConditional(h_batch, g < ctl->ls.nbatches ? 1u : 0u);
-}
-
-// Zero the group's status words and bitmaps, reset the counters and the
-// loop state for the batch; arm the level loop.
-template <int WORDS>
-__global__ void __launch_bounds__(512) k_dl_batch_init(Params p, int g, CondH h_level, CondH) {
-  const GroupBufs gb = p.groups[g];
-  const Team t = make_team(blockIdx.x, gridDim.x);
-  const long long vpad = (p.V + 31) & ~31LL;
-  zero_words(gb.last, vpad * WORDS, t);
-  zero_words(gb.curr, vpad * WORDS, t);
-  zero_words(gb.chg, 2 * p.chg_stride, t);
-  if (t.tid == 0) {
-    Ctl* ctl = gb.ctl;
-    memset(&ctl->par[0], 0, sizeof(Par) * 2);
-    memset(&ctl->qc[0][0], 0, sizeof(ctl->qc));
-    LoopState& ls = ctl->ls;
-    ls.level = 0;
-    ls.dir = kDirTD;
-    ls.max_level = 0;
-    ls.td = ls.bu = 0;
-    ls.m_u = (unsigned long long)p.E;
-    ls.teps = 0;
-    ls.prev_changed = 0;
-    ls.t_lvl = ls.t_mid = global_ns();
-    cudaGraphSetConditional(h_level, 1u);
-  }
-}
-
-template <int WORDS>
-__global__ void __launch_bounds__(512) k_dl_seed(Params p, int g, CondH, CondH) {
-  const GroupBufs gb = p.groups[g];
-  const int b = gb.ctl->ls.batch;
-  seed_phase<WORDS>(p, gb, p.src + (long long)b * p.C, dl_batch_size(p, gb.ctl->ls, b),
-                    make_team(blockIdx.x, gridDim.x));
-}
-
-template <int WORDS>
-__global__ void __launch_bounds__(512) k_dl_inspect(Params p, int g, CondH, CondH) {
-  const GroupBufs gb = p.groups[g];
-  Ctl* ctl = gb.ctl;
-  const int b = ctl->ls.batch, level = ctl->ls.level;
-  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ls.t_mid = global_ns();
-  inspect_phase<WORDS, false>(p, gb, &ctl->par[level & 1], dl_batch_size(p, ctl->ls, b), level,
-                              level <= depth_limit(p.db), false, make_team(blockIdx.x, gridDim.x));
-}
-
-// Top of a level: read the counters of the level just inspected, stop or
-// pick the next direction (choose_dir), write the level record, advance.
-// h_level keeps the level loop running, h_dir selects the expand body
-// (0 top-down, 1 bottom-up, 2 none: the loop ends).
-__global__ void k_dl_decide(Params p, int g, CondH h_level, CondH h_dir) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  Ctl* ctl = p.groups[g].ctl;
-  LoopState& ls = ctl->ls;
-  const int level = ls.level, b = ls.batch;
-  const Par& pr = ctl->par[level & 1];
-  const unsigned long long changed = pr.changed, mf = pr.mf, cdeg = pr.cdeg;
-  ls.teps += pr.teps;
-  ls.m_u = ls.m_u > cdeg ? ls.m_u - cdeg : 0ull;
-  int stop = 0, err = 0;
-  if (pr.range_err) { stop = 1; err = 3; }
-  else if (changed == 0) stop = 1;
-  else if (level + 1 > p.max_levels) { stop = 1; err = 3; }
-  if (changed && !pr.range_err) ls.max_level = level;
-  const int nd = choose_dir(level + 1, ls.dir, p.switch_level, p.alpha, p.beta, changed,
-                            ls.prev_changed, mf, ls.m_u, p.V);
-  ls.prev_changed = changed;
-  const unsigned long long t_now = global_ns();
-  if (level < p.lrec_cap) {
-    LevelRec r;
-    r.batch = b; r.level = level; r.dir = level == 0 ? -1 : ls.dir; r.pad = 0;
-    r.frontier = (long long)changed; r.frontier_edges = (long long)mf;
-    r.expand_ns = (long long)(ls.t_mid - ls.t_lvl);
-    r.inspect_ns = (long long)(t_now - ls.t_mid);
-    p.lrec[(size_t)b * p.lrec_cap + level] = r;
-  }
-  ls.t_lvl = t_now;
-  ls.err = err;
-  if (!stop) {
-    memset((void*)&ctl->par[(level + 1) & 1], 0, sizeof(Par));
-    ctl->qc[level & 1][0] = ctl->qc[level & 1][1] = ctl->qc[level & 1][2] = 0;
-    ls.dir = nd;
-    ls.level = level + 1;
-    if (nd == kDirTD) ls.td++; else ls.bu++;
-  }
-  cudaGraphSetConditional(h_level, stop ? 0u : 1u);
-  cudaGraphSetConditional(h_dir, stop ? 2u : (unsigned)nd);
-}
-
-__global__ void __launch_bounds__(512) k_dl_qbuild(Params p, int g, CondH, CondH) {
-  const GroupBufs gb = p.groups[g];
-  const int level = gb.ctl->ls.level;
-  const Team t = make_team(blockIdx.x, gridDim.x);
-  zero_plane_if_first(p, gb, level, t);
-  qbuild_phase(p, gb, level, gb.ctl->qc[level & 1], t);
-}
-
-template <int WORDS>
-__global__ void __launch_bounds__(512) k_dl_td(Params p, int g, CondH, CondH) {
-  const GroupBufs gb = p.groups[g];
-  const int level = gb.ctl->ls.level;
-  td_phase<WORDS>(p, gb, level, gb.ctl->qc[level & 1], make_team(blockIdx.x, gridDim.x));
-}
-
-template <int WORDS>
-__global__ void __launch_bounds__(512) k_dl_bu(Params p, int g, CondH, CondH) {
-  const GroupBufs gb = p.groups[g];
-  const int level = gb.ctl->ls.level;
-  const Team t = make_team(blockIdx.x, gridDim.x);
-  zero_plane_if_first(p, gb, level, t);
-  bu_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
-                  &gb.ctl->par[level & 1].hq_cnt, t);
-}
-
-template <int WORDS>
-__global__ void __launch_bounds__(512) k_dl_bu_defer(Params p, int g, CondH, CondH) {
-  const GroupBufs gb = p.groups[g];
-  const int level = gb.ctl->ls.level;
-  if (gb.ctl->par[level & 1].hq_cnt == 0) return;  // uniform: nothing deferred
-  bu_defer_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
-                        &gb.ctl->par[level & 1].hq_cnt, make_team(blockIdx.x, gridDim.x));
-}
-
-template <int WORDS>
-__global__ void __launch_bounds__(512) k_dl_output(Params p, int g, CondH, CondH) {
-  __shared__ int32_t s_rows[kMaxWords * 32];
-  const GroupBufs gb = p.groups[g];
-  const LoopState& ls = gb.ctl->ls;
-  if (ls.err) return;  // uniform
-  const int b = ls.batch, n_b = dl_batch_size(p, ls, b);
-  load_rows(p, b, n_b, s_rows);
-  output_phase<WORDS>(p, gb, batch_depth(p, b), s_rows, n_b, ls.max_level,
-                      make_team(blockIdx.x, gridDim.x));
-}
-
-// End of a batch: its record (or the group's error), then the next batch of
-// the group; the batch loop ends after the last one or on an error.
-__global__ void k_dl_batch_end(Params p, int g, CondH h_batch, CondH) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  Ctl* ctl = p.groups[g].ctl;
-  LoopState& ls = ctl->ls;
-  const int b = ls.batch;
-  if (ls.err) {
-    atomicCAS(&ctl->err, 0, ls.err);
-    p.brec[b].err = ls.err;
-    cudaGraphSetConditional(h_batch, 0u);
-    return;
-  }
-  if (ls.level + 1 < p.lrec_cap) {
-    LevelRec r;  // dir 2: the batch's output pass
-    r.batch = b; r.level = ls.level + 1; r.dir = 2; r.pad = 0;
-    r.frontier = 0; r.frontier_edges = 0;
-    r.expand_ns = (long long)(global_ns() - ls.t_lvl);
-    r.inspect_ns = 0;
-    p.lrec[(size_t)b * p.lrec_cap + ls.level + 1] = r;
-  }
-  BatchRec r;
-  r.levels = ls.level;
-  r.max_level = ls.max_level;
-  r.td = ls.td;
-  r.bu = ls.bu;
-  r.teps = ls.teps;
-  r.err = 0;
-  r.pad = 0;
-  p.brec[b] = r;
-  ls.batch = b + p.G;
-  cudaGraphSetConditional(h_batch, ls.batch < ls.nbatches ? 1u : 0u);
 }
 
 // ---------------------------------------------------------------------------
@@ -620,16 +405,6 @@ static const void* persistent_for(int words, int level = 0) {
   }
 }
 
-// Plain schedule: every kernel gets as many CTAs as fit on the GPU for its
-// own register and shared-memory use (a grid-stride team over the whole grid).
-static int occ_grid(const void* fn, int threads, int sms) {
-  int per = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, 0) != cudaSuccess) {
-    (void)cudaGetLastError();
-    per = 1;
-  }
-  return sms * std::max(per, 1);
-}
 
 template <int WORDS>
 static cudaError_t launch_plain_level(const Params& p, const GroupBufs& gb, int sms, int threads,
@@ -665,106 +440,6 @@ static cudaError_t launch_plain_output(const Params& p, const GroupBufs& gb, int
   k_output<WORDS><<<occ_grid((const void*)k_output<WORDS>, threads, sms), threads, 0, s>>>(
       p, gb, b, max_level);
   return cudaGetLastError();
-}
-
-#define DISPATCH_WORDS(words, fn, ...)                  \
-  ((words) == 1   ? fn<1>(__VA_ARGS__)                  \
-   : (words) == 2 ? fn<2>(__VA_ARGS__)                  \
-   : (words) == 4 ? fn<4>(__VA_ARGS__)                  \
-                  : fn<8>(__VA_ARGS__))
-
-// ---- device-driven schedule: graph construction ------------------------
-using DlKernel = void (*)(Params, int, CondH, CondH);
-
-static cudaError_t dl_kernel(cudaGraph_t gr, cudaGraphNode_t* out, cudaGraphNode_t dep,
-                             DlKernel fn, int grid, int threads, const Params& p, int g,
-                             CondH h0, CondH h1) {
-  Params pp = p;
-  int gg = g;
-  CondH a = h0, b = h1;
-  void* args[] = {&pp, &gg, &a, &b};
-  cudaKernelNodeParams kp;
-  std::memset(&kp, 0, sizeof(kp));
-  kp.func = reinterpret_cast<void*>(fn);
-  kp.gridDim = dim3((unsigned)grid);
-  kp.blockDim = dim3((unsigned)threads);
-  kp.kernelParams = args;
-  return cudaGraphAddKernelNode(out, gr, dep ? &dep : nullptr, dep ? 1 : 0, &kp);
-}
-
-static cudaError_t dl_cond(cudaGraph_t gr, cudaGraphNode_t* out, cudaGraphNode_t dep, CondH h,
-                           cudaGraphConditionalNodeType type, unsigned size, cudaGraph_t* bodies) {
-  cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
-  np.conditional.handle = h;
-  np.conditional.type = type;
-  np.conditional.size = size;
-  cudaError_t e = cudaGraphAddNode(out, gr, dep ? &dep : nullptr, dep ? 1 : 0, &np);
-  if (e == cudaSuccess)
-    for (unsigned i = 0; i < size; i++) bodies[i] = np.conditional.phGraph_out[i];
-  return e;
-}
-
-// One branch per group g:
-//   start -> WHILE(batch) { init -> seed -> inspect(0) -> WHILE(level) {
-//              decide -> SWITCH(dir) { 0: qbuild -> td -> inspect,
-//                                      1: bu -> bu_defer -> inspect } }
-//            -> output -> batch_end }
-// Every loop ends: decide stops at an empty level or past max_levels, and
-// batch_end stops after the group's last batch or on an error.
-template <int WORDS>
-static cudaError_t build_device_loop(const Params& p, int G, int sms, int threads,
-                                     cudaGraph_t* out) {
-  *out = nullptr;
-  cudaGraph_t top = nullptr;
-  cudaError_t e = cudaGraphCreate(&top, 0);
-  if (e != cudaSuccess) return e;
-  const int gz = occ_grid((const void*)k_dl_batch_init<WORDS>, threads, sms);
-  const int gi = occ_grid((const void*)k_dl_inspect<WORDS>, threads, sms);
-  const int gq = occ_grid((const void*)k_dl_qbuild, threads, sms);
-  const int gt = occ_grid((const void*)k_dl_td<WORDS>, threads, sms);
-  const int gu = occ_grid((const void*)k_dl_bu<WORDS>, threads, sms);
-  const int gd = occ_grid((const void*)k_dl_bu_defer<WORDS>, threads, sms);
-  const int go = occ_grid((const void*)k_dl_output<WORDS>, threads, sms);
-#define DL_TRY(call)                   \
-  do {                                 \
-    e = (call);                        \
-    if (e != cudaSuccess) {            \
-      cudaGraphDestroy(top);           \
-      return e;                        \
-    }                                  \
-  } while (0)
-  for (int g = 0; g < G; g++) {
-    CondH hb = 0, hl = 0, hd = 0;
-    DL_TRY(cudaGraphConditionalHandleCreate(&hb, top, 0, cudaGraphCondAssignDefault));
-    cudaGraphNode_t n0, n1;
-    DL_TRY(dl_kernel(top, &n0, nullptr, k_dl_start, 1, 32, p, g, hb, 0));
-    cudaGraph_t B = nullptr;
-    DL_TRY(dl_cond(top, &n1, n0, hb, cudaGraphCondTypeWhile, 1, &B));
-    DL_TRY(cudaGraphConditionalHandleCreate(&hl, B, 0, cudaGraphCondAssignDefault));
-    cudaGraphNode_t b0, b1, b2, b3, b4, b5;
-    DL_TRY(dl_kernel(B, &b0, nullptr, k_dl_batch_init<WORDS>, gz, threads, p, g, hl, 0));
-    DL_TRY(dl_kernel(B, &b1, b0, k_dl_seed<WORDS>, 1, 512, p, g, 0, 0));
-    DL_TRY(dl_kernel(B, &b2, b1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
-    cudaGraph_t L = nullptr;
-    DL_TRY(dl_cond(B, &b3, b2, hl, cudaGraphCondTypeWhile, 1, &L));
-    DL_TRY(dl_kernel(B, &b4, b3, k_dl_output<WORDS>, go, threads, p, g, 0, 0));
-    DL_TRY(dl_kernel(B, &b5, b4, k_dl_batch_end, 1, 32, p, g, hb, 0));
-    DL_TRY(cudaGraphConditionalHandleCreate(&hd, L, 2, cudaGraphCondAssignDefault));
-    cudaGraphNode_t l0, l1;
-    DL_TRY(dl_kernel(L, &l0, nullptr, k_dl_decide, 1, 32, p, g, hl, hd));
-    cudaGraph_t S[2] = {nullptr, nullptr};
-    DL_TRY(dl_cond(L, &l1, l0, hd, cudaGraphCondTypeSwitch, 2, S));
-    cudaGraphNode_t t0, t1, t2, u0, u1, u2;
-    DL_TRY(dl_kernel(S[0], &t0, nullptr, k_dl_qbuild, gq, threads, p, g, 0, 0));
-    DL_TRY(dl_kernel(S[0], &t1, t0, k_dl_td<WORDS>, gt, threads, p, g, 0, 0));
-    DL_TRY(dl_kernel(S[0], &t2, t1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
-    DL_TRY(dl_kernel(S[1], &u0, nullptr, k_dl_bu<WORDS>, gu, threads, p, g, 0, 0));
-    DL_TRY(dl_kernel(S[1], &u1, u0, k_dl_bu_defer<WORDS>, gd, threads, p, g, 0, 0));
-    DL_TRY(dl_kernel(S[1], &u2, u1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
-  }
-#undef DL_TRY
-  *out = top;
-  return cudaSuccess;
 }
 
 struct RunPlan {
@@ -1293,7 +968,9 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   p.hub_t = kHubScan;
   p.bu_filter = o.bu_filter > 0 ? 1 : 0;
   p.col_vec = 1;
-  p.vec_sm = (g->V % 4 == 0) && ((reinterpret_cast<uintptr_t>(dout) & 3) == 0);
+  p.vec_sm = (g->V % 16 == 0 && (reinterpret_cast<uintptr_t>(dout) & 15) == 0)  ? 16
+             : (g->V % 4 == 0 && (reinterpret_cast<uintptr_t>(dout) & 3) == 0) ? 4
+                                                                              : 0;
 
   int64_t launches = 0;
   const bool use_graph = persistent && o.use_graph && !o.debug_withhold;
@@ -1398,8 +1075,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     if (!(g->dlcache.exec && g->dlcache.key == key)) {
       g->dlcache.release();
       cudaGraph_t graph = nullptr;
-      cudaError_t be = DISPATCH_WORDS(rp.words, build_device_loop, p, rp.G, g->sms, rp.threads,
-                                      &graph);
+      cudaError_t be = build_device_loop_graph(p, rp.words, rp.G, g->sms, rp.threads, &graph);
       if (be != cudaSuccess) {
         last_cuda_error() = be;
         (void)cudaGetLastError();

@@ -49,6 +49,9 @@ struct Params;
 cudaError_t launch_persistent_params(const Params& p, int words, int grid, int threads,
                                      size_t smem, cudaStream_t s);
 cudaError_t persistent_occupancy(int words, int threads, size_t smem, int* per_sm);
+// devloop.cu: the device-loop CUDA graph of one run (not instantiated).
+cudaError_t build_device_loop_graph(const Params& p, int words, int G, int sms, int threads,
+                                    cudaGraph_t* out);
 }  // namespace ibfs
 
 namespace ibfs {
