@@ -459,7 +459,12 @@ def run_serving(args, cfg):
                                depth_bytes=1)
         base = sb.run_one_per_launch(g, qs, arr, width=args.width)
         sweep.append({"rate_qps": rate, "served": served, "one_query_per_launch": base})
-    top = max(sweep, key=lambda x: x["served"]["gteps"])
+    # the headline point is the highest-throughput rate that meets the
+    # latency objective (p99 <= --slo-p99-ms); beyond it latency is queueing,
+    # reported apart as the saturated capacity
+    ok = [x for x in sweep if x["served"]["p99_ms"] <= args.slo_p99_ms] or sweep[:1]
+    top = max(ok, key=lambda x: x["served"]["gteps"])
+    cap = max(sweep, key=lambda x: x["served"]["gteps"])
     line = {
         "metric": "aggregate GTEPS under Poisson load (served); p50/p99 query latency",
         "value": round(top["served"]["gteps"], 3), "unit": "GTEPS", "n_gpus": 1,
@@ -469,9 +474,14 @@ def run_serving(args, cfg):
         "config": {"workload": cfg["workload"], "V": int(len(beg) - 1), "E": int(len(col)),
                    "query_sources": "1-256 log-uniform", "width": args.width,
                    "round_batches": args.round_batches, "max_wait_us": args.max_wait_us,
-                   "latency": "submission to depths complete in HBM"},
+                   "latency": "submission to depths complete in HBM",
+                   "slo_p99_ms": args.slo_p99_ms},
         "p50_ms": round(top["served"]["p50_ms"], 3), "p99_ms": round(top["served"]["p99_ms"], 3),
-        "rate_qps": top["rate_qps"], "sweep": sweep,
+        "rate_qps": top["rate_qps"],
+        "saturated": {"gteps": round(cap["served"]["gteps"], 3), "rate_qps": cap["rate_qps"],
+                      "p50_ms": round(cap["served"]["p50_ms"], 3),
+                      "p99_ms": round(cap["served"]["p99_ms"], 3)},
+        "sweep": sweep,
     }
     print(json.dumps(line), flush=True)
     g.close()
@@ -496,10 +506,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=10.0)
-    ap.add_argument("--rates", default="100,1000,3000,10000")
+    ap.add_argument("--rates", default="100,1000,2000,3000")
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--max-queries", type=int, default=3000)
     ap.add_argument("--round-batches", type=int, default=4)
+    ap.add_argument("--slo-p99-ms", type=float, default=50.0)
     ap.add_argument("--max-wait-us", type=int, default=500)
     args = ap.parse_args()
     cfg = CONFIGS[args.config]

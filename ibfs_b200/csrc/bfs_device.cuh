@@ -137,6 +137,12 @@ struct Params {
                     // a hub still missing bits defers the rest in chunks
 };
 
+// Neighbours one thread of the bottom-up thread path has in flight per step
+// (4 or 8).
+#ifndef IBFS_BU_STEP
+#define IBFS_BU_STEP 4
+#endif
+constexpr int kBuStep = IBFS_BU_STEP;
 constexpr int kHubScan = 1024;   // neighbours one warp scans before deferring
 constexpr int kHubChunk = 2048;  // edges per deferred chunk (one CTA each)
 
@@ -788,28 +794,34 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
     need = need && valid && (b1 > b0);
     const bool small = need && (b1 - b0) <= p.but;
     if (small) {
-      // four neighbours in flight per step; with col_vec their ids are one
-      // aligned 16-byte vector (col is padded by 4 entries at its end)
+      // kBuStep neighbours in flight per step; with col_vec their ids come as
+      // aligned 16-byte vectors (col is padded by 4 entries at its end, and
+      // a vector is only read when it starts before b1)
+      constexpr int S = kBuStep;
       const int4* col4 = reinterpret_cast<const int4*>(p.col);
       const long long a0 = p.col_vec ? (b0 & ~3LL) : b0;
-      for (long long a = a0; a < b1; a += 4) {
-        int32_t u[4];
+      for (long long a = a0; a < b1; a += S) {
+        int32_t u[S];
         if (p.col_vec) {
-          const int4 c4 = __ldg(col4 + (a >> 2));
-          u[0] = c4.x; u[1] = c4.y; u[2] = c4.z; u[3] = c4.w;
+#pragma unroll
+          for (int q = 0; q < S / 4; q++) {
+            int4 c4 = make_int4(0, 0, 0, 0);
+            if (q == 0 || a + 4 * q < b1) c4 = __ldg(col4 + ((a >> 2) + q));
+            u[4 * q] = c4.x; u[4 * q + 1] = c4.y; u[4 * q + 2] = c4.z; u[4 * q + 3] = c4.w;
+          }
         } else {
 #pragma unroll
-          for (int i = 0; i < 4; i++) u[i] = a + i < b1 ? __ldg(p.col + a + i) : 0;
+          for (int i = 0; i < S; i++) u[i] = a + i < b1 ? __ldg(p.col + a + i) : 0;
         }
-        bool f[4];
+        bool f[S];
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
+        for (int i = 0; i < S; i++) {
           const bool in = (a + i >= b0) && (a + i < b1);
           f[i] = in && (!p.bu_filter || ((__ldcg(front + (u[i] >> 5)) >> (u[i] & 31)) & 1u));
         }
-        uint32_t x[4][WORDS];
+        uint32_t x[S][WORDS];
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
+        for (int i = 0; i < S; i++) {
           if (f[i]) {
             ld_status<WORDS>(gb.last + (size_t)u[i] * WORDS, x[i]);
           } else {
@@ -820,7 +832,8 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
         bool miss = false;
 #pragma unroll
         for (int k = 0; k < WORDS; k++) {
-          acc[k] |= x[0][k] | x[1][k] | x[2][k] | x[3][k];
+#pragma unroll
+          for (int i = 0; i < S; i++) acc[k] |= x[i][k];
           miss |= (fm[k] & ~acc[k]) != 0u;
         }
         if (!miss) break;

@@ -343,7 +343,11 @@ struct ibfs_graph {
   DevBuf d_groups, d_src, d_outrow, d_brec, d_lrec, d_out;
   PinBuf h_src, h_outrow, h_brec, h_lrec, h_par;
   GraphCache gcache;
-  GraphCache dlcache;  // device-driven schedule: keyed by the launch Params
+  // device-loop graphs, keyed by the launch Params: a few entries, because a
+  // server's rounds alternate between group counts (1..4 batches per round)
+  static constexpr int kDlCache = 4;
+  GraphCache dlcache[kDlCache];
+  unsigned dl_next = 0;
   std::mutex mu;
 };
 
@@ -367,6 +371,7 @@ static ibfs_status check_opts(const ibfs_opts* o) {
   if (o->sml_shed < 1 || o->lrg_shed < o->sml_shed - 1) return IBFS_ERR_INVALID_ARG;
   if (o->groups < 0 || o->ctas_per_sm < 0 || o->timeout_ms < 0 || o->max_levels < 0)
     return IBFS_ERR_INVALID_ARG;
+  if (o->bu_thread_max < 0 || o->bu_thread_max > (1 << 20)) return IBFS_ERR_INVALID_ARG;
   return IBFS_OK;
 }
 
@@ -534,6 +539,7 @@ extern "C" void ibfs_opts_default(ibfs_opts* o) {
   o->debug_withhold = 0;
   o->occupancy = 0;
   o->bu_filter = -1;  // default: off (measured faster on B200)
+  o->bu_thread_max = 32;
 }
 
 static ibfs_status upload_graph(ibfs_graph* g) {
@@ -608,7 +614,7 @@ static void destroy_graph(ibfs_graph* g) {
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
   g->gcache.release();
-  g->dlcache.release();
+  for (auto& c : g->dlcache) c.release();
   for (auto& m : g->groups) m.release();
   g->beg.release();
   g->col.release();
@@ -953,7 +959,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   p.sml = o.sml_shed;
   p.lrg = o.lrg_shed;
   p.chunk = rp.threads * 4;
-  p.but = 32;
+  p.but = o.bu_thread_max > 0 ? o.bu_thread_max : 32;
   p.switch_level = o.switch_level;
   p.alpha = o.alpha;
   p.beta = o.beta;
@@ -1072,8 +1078,12 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     std::string key(reinterpret_cast<const char*>(&pk), sizeof(pk));
     const int shape[4] = {rp.G, rp.threads, g->sms, rp.words};
     key.append(reinterpret_cast<const char*>(shape), sizeof(shape));
-    if (!(g->dlcache.exec && g->dlcache.key == key)) {
-      g->dlcache.release();
+    GraphCache* slot = nullptr;
+    for (auto& c : g->dlcache)
+      if (c.exec && c.key == key) slot = &c;
+    if (!slot) {
+      slot = &g->dlcache[g->dl_next++ % ibfs_graph::kDlCache];
+      slot->release();
       cudaGraph_t graph = nullptr;
       cudaError_t be = build_device_loop_graph(p, rp.words, rp.G, g->sms, rp.threads, &graph);
       if (be != cudaSuccess) {
@@ -1089,11 +1099,11 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
         (void)cudaGetLastError();
         return IBFS_ERR_CUDA;
       }
-      g->dlcache.exec = exec;
-      g->dlcache.key = key;
+      slot->exec = exec;
+      slot->key = key;
     }
     CU(cudaEventRecord(g->ev0, s));
-    CU(cudaGraphLaunch(g->dlcache.exec, s));
+    CU(cudaGraphLaunch(slot->exec, s));
     CU(cudaEventRecord(g->ev1, s));
     if (rp.host_out) CU(cudaMemcpyAsync(depth_out, dout, out_bytes, cudaMemcpyDeviceToHost, s));
   } else {

@@ -109,7 +109,9 @@ typedef struct ibfs_opts {
                               previous frontier bitmap has it: 1 on, 0 or -1 off
                               (the default: the bitmap lookup costs more than the
                               status reads it saves)                              */
-    int32_t reserved[5];
+    int32_t bu_thread_max; /* bottom-up: vertices of degree <= this scan alone, one
+                              thread each; above it a warp scans (0: 32)          */
+    int32_t reserved[4];
 } ibfs_opts;
 
 typedef struct ibfs_level_rec {
