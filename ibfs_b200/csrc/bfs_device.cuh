@@ -62,6 +62,9 @@ struct LoopState {
   int32_t max_level;
   int32_t td, bu;
   int32_t err;
+  int32_t flip;       // 1: the status "last" lives in GroupBufs::curr and vice versa
+  int32_t sync;       // the next top-down level first copies new statuses over old ones
+  int32_t pad;
   unsigned long long m_u, teps, prev_changed;
   unsigned long long t_lvl, t_mid;  // %globaltimer at the level start / inspect start
 };
@@ -529,8 +532,12 @@ __host__ __device__ inline bool inspect_dense(unsigned long long prev_mf, long l
 // medium, deg 0 dropped).  Large vertices are cut into chunks of p.chunk
 // edges.  Clears the level-L bitmap that the top-down pass will fill.
 // ---------------------------------------------------------------------------
+// With `sync` (a top-down level right after a fused bottom-up level, which
+// left the new statuses in `last` and the previous ones in `curr`) every
+// changed vertex also copies last -> curr, restoring curr == last.
+template <int WORDS = 4>
 __device__ inline void qbuild_phase(const Params& p, const GroupBufs& gb, int level,
-                                    int32_t* qc, const Team& t) {
+                                    int32_t* qc, const Team& t, bool sync = false) {
   const int lane = t.lane;
   const uint32_t lt = (1u << lane) - 1u;
   const uint32_t* prev = chg_at(gb, p, level - 1);
@@ -555,6 +562,11 @@ __device__ inline void qbuild_phase(const Params& p, const GroupBufs& gb, int le
     const bool mine = (bits >> lane) & 1u;
     long long deg = 0;
     if (mine) deg = p.beg[v + 1] - p.beg[v];
+    if (sync && mine) {
+      uint32_t x[WORDS];
+      ld_status<WORDS>(gb.last + (size_t)v * WORDS, x);
+      st_status<WORDS>(gb.curr + (size_t)v * WORDS, x);
+    }
     const int cls = (!mine || deg == 0) ? -1 : deg < p.sml ? 0 : deg <= p.lrg ? 1 : 2;
     const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, cls == 0);
     if (m0) {
@@ -763,15 +775,37 @@ __device__ void bu_defer_phase(const Params& p, const GroupBufs& gb, int level,
 // 431-489), the rest with the whole warp and a warp OR-reduction
 // (sw_expand_warp, expander.cuh:341-422).
 // ---------------------------------------------------------------------------
-template <int WORDS>
+//
+// FUSED (device loop only) also does the inspect work of the level in the
+// same pass, so that bottom-up levels need no inspect pass: every vertex's
+// new status goes to `curr` (for all vertices, changed or not: `curr` then
+// holds the complete status of the level while `last` keeps the previous
+// one, and the caller swaps their roles), the new bits update the depth
+// planes and the counters directly (the whole plane b is written at level
+// 2^b, so it needs no zeroing), and the changed bitmap is still marked for a
+// following top-down level.  Hubs deferred to bu_defer_phase get their
+// planes and counters in bu_hub_epilogue.
+template <int WORDS, bool FUSED = false>
 __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
-                         const uint32_t* fmask_g, int32_t* hq_cnt, const Team& t) {
+                         const uint32_t* fmask_g, int32_t* hq_cnt, const Team& t,
+                         Par* par = nullptr, int n_b = 0, bool depth_ok = true) {
   uint32_t fm[WORDS];
 #pragma unroll
   for (int k = 0; k < WORDS; k++) fm[k] = __ldcg(fmask_g + k);
   const uint32_t* front = chg_at(gb, p, level - 1);
   uint32_t* out = chg_at(gb, p, level);
   const int lane = t.lane;
+  // FUSED counters (as inspect_phase)
+  unsigned long long f_mf = 0, f_cnt = 0, f_cdeg = 0, f_teps = 0;
+  uint32_t f_fm[WORDS], full[WORDS];
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) {
+    f_fm[k] = 0;
+    full[k] = full_word(n_b, k);
+  }
+  const bool first_plane = (level & (level - 1)) == 0;
+  const int pb = __ffs(level) - 1;
+  bool range = false;
   for (long long base = t.warp * 32; base < p.V; base += t.nwarps * 32) {
     const long long v = base + lane;
     const bool valid = v < p.V;
@@ -839,6 +873,7 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
         if (!miss) break;
       }
     }
+    bool deferred = false;  // this lane's vertex left chunks to bu_defer_phase
     uint32_t big = __ballot_sync(0xFFFFFFFFu, need && !small);
     while (big) {
       const int j = __ffs(big) - 1;
@@ -869,7 +904,8 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
         }
         if (!miss) break;
       }
-      if (miss && e_lim < e1 && lane == 0) {
+      const bool defer = miss && e_lim < e1;
+      if (defer && lane == 0) {
         const int nch = (int)((e1 - e_lim + kHubChunk - 1) / kHubChunk);
         const int base0 = atomicAdd(hq_cnt, nch);
         for (int c = 0; c < nch; c++) gb.hq[base0 + c] = make_int2((int)(base + j), c);
@@ -877,16 +913,131 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
       if (lane == j) {
 #pragma unroll
         for (int k = 0; k < WORDS; k++) acc[k] = a[k];
+        deferred = defer;
       }
     }
     bool ch = false;
 #pragma unroll
     for (int k = 0; k < WORDS; k++) ch |= acc[k] != l[k];
     ch = ch && need;
-    if (ch) st_status<WORDS>(gb.curr + (size_t)v * WORDS, acc);
+    if constexpr (!FUSED) {
+      if (ch) st_status<WORDS>(gb.curr + (size_t)v * WORDS, acc);
+    } else if (valid) {
+      st_status<WORDS>(gb.curr + (size_t)v * WORDS, acc);  // every vertex: curr = new status
+      const bool epi = ch && !deferred;  // deferred hubs: bu_hub_epilogue
+      uint32_t nb[WORDS];
+      uint32_t pop = 0;
+      bool comp = true;
+#pragma unroll
+      for (int k = 0; k < WORDS; k++) {
+        nb[k] = epi ? (acc[k] & ~l[k]) : 0u;
+        pop += __popc(nb[k]);
+        comp = comp && acc[k] == full[k];
+        f_fm[k] |= nb[k];
+      }
+      if (epi) {
+        const unsigned long long deg = (unsigned long long)(b1 - b0);
+        f_cnt += 1;
+        f_mf += deg;
+        f_teps += deg * pop;
+        if (comp) f_cdeg += deg;
+        if (!depth_ok) range = true;
+      }
+      uint32_t* q0 = gb.planes + (size_t)v * WORDS;
+      if (first_plane) {
+        // level 2^b is the first to use plane b: write it whole (0 where no bit is new)
+        st_status<WORDS>(q0 + (size_t)pb * p.plane_stride, nb);
+      } else if (epi && depth_ok) {
+        unsigned rest = (unsigned)level;
+        while (rest) {
+          const int b0p = __ffs(rest) - 1;
+          rest &= rest - 1;
+          uint32_t* qa = q0 + (size_t)b0p * p.plane_stride;
+          uint32_t xa[WORDS];
+          ld_status<WORDS>(qa, xa);
+#pragma unroll
+          for (int k = 0; k < WORDS; k++) xa[k] |= nb[k];
+          st_status<WORDS>(qa, xa);
+        }
+      }
+      ch = epi;
+    }
     const uint32_t bal = __ballot_sync(0xFFFFFFFFu, ch);
     if (lane == 0 && bal) atomicOr(out + (base >> 5), bal);
   }
+  if constexpr (FUSED) {
+    if (range) par->range_err = 1;
+    cta_add_u64(&par->changed, f_cnt);
+    cta_add_u64(&par->mf, f_mf);
+    cta_add_u64(&par->cdeg, f_cdeg);
+    cta_add_u64(&par->teps, f_teps);
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) cta_or_u32(&par->fmask[k], f_fm[k]);
+  }
+}
+
+// FUSED bottom-up, after bu_defer_phase: the inspect work of the hubs whose
+// scan was deferred (one entry per hub: chunk 0), from their final status
+// in `curr` and the previous one in `last`; and the level+1 bitmap cleared
+// for the next expand (what inspect_phase does on other levels).
+template <int WORDS>
+__device__ void bu_hub_epilogue(const Params& p, const GroupBufs& gb, Par* par, int n_b,
+                                int level, bool depth_ok, const Team& t) {
+  zero_words(chg_at(gb, p, level + 1), p.chg_stride, t);
+  uint32_t full[WORDS], fm[WORDS];
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) {
+    full[k] = full_word(n_b, k);
+    fm[k] = 0;
+  }
+  unsigned long long mf = 0, cnt = 0, cdeg = 0, teps = 0;
+  uint32_t* out = chg_at(gb, p, level);
+  const int n = __ldcg(&par->hq_cnt);
+  for (long long i = t.tid; i < n; i += t.nthreads) {
+    const int2 hc = gb.hq[i];
+    if (hc.y != 0) continue;
+    const long long v = hc.x;
+    uint32_t c[WORDS], l[WORDS], nb[WORDS];
+    ld_status<WORDS>(gb.curr + (size_t)v * WORDS, c);
+    ld_status<WORDS>(gb.last + (size_t)v * WORDS, l);
+    bool any = false, comp = true;
+    uint32_t pop = 0;
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) {
+      nb[k] = c[k] & ~l[k];
+      any |= nb[k] != 0u;
+      comp = comp && c[k] == full[k];
+      pop += __popc(nb[k]);
+      fm[k] |= nb[k];
+    }
+    if (!any) continue;
+    const unsigned long long deg = (unsigned long long)(p.beg[v + 1] - p.beg[v]);
+    cnt += 1;
+    mf += deg;
+    teps += deg * pop;
+    if (comp) cdeg += deg;
+    if (!depth_ok) par->range_err = 1;
+    atomicOr(out + (v >> 5), 1u << (v & 31));
+    if (depth_ok) {
+      unsigned rest = (unsigned)level;
+      while (rest) {
+        const int b = __ffs(rest) - 1;
+        rest &= rest - 1;
+        uint32_t* q = gb.planes + (size_t)b * p.plane_stride + (size_t)v * WORDS;
+        uint32_t x[WORDS];
+        ld_status<WORDS>(q, x);
+#pragma unroll
+        for (int k = 0; k < WORDS; k++) x[k] |= nb[k];
+        st_status<WORDS>(q, x);
+      }
+    }
+  }
+  cta_add_u64(&par->changed, cnt);
+  cta_add_u64(&par->mf, mf);
+  cta_add_u64(&par->cdeg, cdeg);
+  cta_add_u64(&par->teps, teps);
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) cta_or_u32(&par->fmask[k], fm[k]);
 }
 
 // ---------------------------------------------------------------------------

@@ -54,6 +54,23 @@ __device__ __forceinline__ int dl_batch_size(const Params& p, const LoopState& l
   return (int)min((long long)p.C, ls.n_total - (long long)b * p.C);
 }
 
+// Bottom-up levels run fused with their inspect work (bu_phase<.., true>):
+// they write every vertex's new status into the buffer that is not `last`,
+// and the decision kernel then swaps the two buffers' roles (LoopState::flip)
+// instead of copying.  Every kernel sees the buffers through dl_bufs.
+#ifndef IBFS_DL_FUSED_BU
+#define IBFS_DL_FUSED_BU 1
+#endif
+__device__ __forceinline__ GroupBufs dl_bufs(const Params& p, int g) {
+  GroupBufs gb = p.groups[g];
+  if (gb.ctl->ls.flip) {
+    uint32_t* x = gb.last;
+    gb.last = gb.curr;
+    gb.curr = x;
+  }
+  return gb;
+}
+
 // First batch of group g; the batch loop runs while it exists.
 __global__ void k_dl_start(Params p, int g, CondH h_batch, CondH) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -85,6 +102,8 @@ __global__ void __launch_bounds__(512) k_dl_batch_init(Params p, int g, CondH h_
     ls.m_u = (unsigned long long)p.E;
     ls.teps = 0;
     ls.prev_changed = 0;
+    ls.flip = 0;
+    ls.sync = 0;
     ls.t_lvl = ls.t_mid = global_ns();
     cudaGraphSetConditional(h_level, 1u);
   }
@@ -92,7 +111,7 @@ __global__ void __launch_bounds__(512) k_dl_batch_init(Params p, int g, CondH h_
 
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_dl_seed(Params p, int g, CondH, CondH) {
-  const GroupBufs gb = p.groups[g];
+  const GroupBufs gb = dl_bufs(p, g);
   const int b = gb.ctl->ls.batch;
   seed_phase<WORDS>(p, gb, p.src + (long long)b * p.C, dl_batch_size(p, gb.ctl->ls, b),
                     make_team(blockIdx.x, gridDim.x));
@@ -100,7 +119,7 @@ __global__ void __launch_bounds__(512) k_dl_seed(Params p, int g, CondH, CondH) 
 
 template <int WORDS>
 __global__ void DL_INSPECT_BOUNDS k_dl_inspect(Params p, int g, CondH, CondH) {
-  const GroupBufs gb = p.groups[g];
+  const GroupBufs gb = dl_bufs(p, g);
   Ctl* ctl = gb.ctl;
   const int b = ctl->ls.batch, level = ctl->ls.level;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ls.t_mid = global_ns();
@@ -117,6 +136,9 @@ __global__ void k_dl_decide(Params p, int g, CondH h_level, CondH h_dir) {
   Ctl* ctl = p.groups[g].ctl;
   LoopState& ls = ctl->ls;
   const int level = ls.level, b = ls.batch;
+  // a fused bottom-up level left its statuses in the other buffer
+  const bool was_bu = IBFS_DL_FUSED_BU && level > 0 && ls.dir == kDirBU;
+  if (was_bu) ls.flip ^= 1;
   const Par& pr = ctl->par[level & 1];
   const unsigned long long changed = pr.changed, mf = pr.mf, cdeg = pr.cdeg;
   ls.teps += pr.teps;
@@ -143,6 +165,7 @@ __global__ void k_dl_decide(Params p, int g, CondH h_level, CondH h_dir) {
   if (!stop) {
     memset((void*)&ctl->par[(level + 1) & 1], 0, sizeof(Par));
     ctl->qc[level & 1][0] = ctl->qc[level & 1][1] = ctl->qc[level & 1][2] = 0;
+    ls.sync = (was_bu && nd == kDirTD) ? 1 : 0;  // top-down needs curr == last again
     ls.dir = nd;
     ls.level = level + 1;
     if (nd == kDirTD) ls.td++; else ls.bu++;
@@ -151,34 +174,53 @@ __global__ void k_dl_decide(Params p, int g, CondH h_level, CondH h_dir) {
   cudaGraphSetConditional(h_dir, stop ? 2u : (unsigned)nd);
 }
 
+template <int WORDS>
 __global__ void __launch_bounds__(512) k_dl_qbuild(Params p, int g, CondH, CondH) {
-  const GroupBufs gb = p.groups[g];
+  const GroupBufs gb = dl_bufs(p, g);
   const int level = gb.ctl->ls.level;
   const Team t = make_team(blockIdx.x, gridDim.x);
   zero_plane_if_first(p, gb, level, t);
-  qbuild_phase(p, gb, level, gb.ctl->qc[level & 1], t);
+  qbuild_phase<WORDS>(p, gb, level, gb.ctl->qc[level & 1], t, gb.ctl->ls.sync != 0);
 }
 
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_dl_td(Params p, int g, CondH, CondH) {
-  const GroupBufs gb = p.groups[g];
+  const GroupBufs gb = dl_bufs(p, g);
   const int level = gb.ctl->ls.level;
   td_phase<WORDS>(p, gb, level, gb.ctl->qc[level & 1], make_team(blockIdx.x, gridDim.x));
 }
 
 template <int WORDS>
 __global__ void DL_BU_BOUNDS k_dl_bu(Params p, int g, CondH, CondH) {
-  const GroupBufs gb = p.groups[g];
-  const int level = gb.ctl->ls.level;
+  const GroupBufs gb = dl_bufs(p, g);
+  const LoopState& ls = gb.ctl->ls;
+  const int level = ls.level;
   const Team t = make_team(blockIdx.x, gridDim.x);
-  zero_plane_if_first(p, gb, level, t);
-  bu_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
-                  &gb.ctl->par[level & 1].hq_cnt, t);
+  if (IBFS_DL_FUSED_BU) {
+    bu_phase<WORDS, true>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
+                          &gb.ctl->par[level & 1].hq_cnt, t, &gb.ctl->par[level & 1],
+                          dl_batch_size(p, ls, ls.batch), level <= depth_limit(p.db));
+  } else {
+    zero_plane_if_first(p, gb, level, t);
+    bu_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
+                    &gb.ctl->par[level & 1].hq_cnt, t);
+  }
+}
+
+// The inspect step of a fused bottom-up level: deferred hubs only.
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_dl_bu_hubs(Params p, int g, CondH, CondH) {
+  const GroupBufs gb = dl_bufs(p, g);
+  Ctl* ctl = gb.ctl;
+  const int b = ctl->ls.batch, level = ctl->ls.level;
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ls.t_mid = global_ns();
+  bu_hub_epilogue<WORDS>(p, gb, &ctl->par[level & 1], dl_batch_size(p, ctl->ls, b), level,
+                         level <= depth_limit(p.db), make_team(blockIdx.x, gridDim.x));
 }
 
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_dl_bu_defer(Params p, int g, CondH, CondH) {
-  const GroupBufs gb = p.groups[g];
+  const GroupBufs gb = dl_bufs(p, g);
   const int level = gb.ctl->ls.level;
   if (gb.ctl->par[level & 1].hq_cnt == 0) return;  // uniform: nothing deferred
   bu_defer_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
@@ -188,7 +230,7 @@ __global__ void __launch_bounds__(512) k_dl_bu_defer(Params p, int g, CondH, Con
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_dl_output(Params p, int g, CondH, CondH) {
   __shared__ int32_t s_rows[kMaxWords * 32];
-  const GroupBufs gb = p.groups[g];
+  const GroupBufs gb = dl_bufs(p, g);
   const LoopState& ls = gb.ctl->ls;
   if (ls.err) return;  // uniform
   const int b = ls.batch, n_b = dl_batch_size(p, ls, b);
@@ -278,7 +320,8 @@ static cudaError_t build_device_loop(const Params& p, int G, int sms, int thread
   if (e != cudaSuccess) return e;
   const int gz = occ_grid((const void*)k_dl_batch_init<WORDS>, threads, sms);
   const int gi = occ_grid((const void*)k_dl_inspect<WORDS>, threads, sms);
-  const int gq = occ_grid((const void*)k_dl_qbuild, threads, sms);
+  const int gq = occ_grid((const void*)k_dl_qbuild<WORDS>, threads, sms);
+  const int gh = occ_grid((const void*)k_dl_bu_hubs<WORDS>, threads, sms);
   const int gt = occ_grid((const void*)k_dl_td<WORDS>, threads, sms);
   const int gu = occ_grid((const void*)k_dl_bu<WORDS>, threads, sms);
   const int gd = occ_grid((const void*)k_dl_bu_defer<WORDS>, threads, sms);
@@ -313,12 +356,15 @@ static cudaError_t build_device_loop(const Params& p, int G, int sms, int thread
     cudaGraph_t S[2] = {nullptr, nullptr};
     DL_TRY(dl_cond(L, &l1, l0, hd, cudaGraphCondTypeSwitch, 2, S));
     cudaGraphNode_t t0, t1, t2, u0, u1, u2;
-    DL_TRY(dl_kernel(S[0], &t0, nullptr, k_dl_qbuild, gq, threads, p, g, 0, 0));
+    DL_TRY(dl_kernel(S[0], &t0, nullptr, k_dl_qbuild<WORDS>, gq, threads, p, g, 0, 0));
     DL_TRY(dl_kernel(S[0], &t1, t0, k_dl_td<WORDS>, gt, threads, p, g, 0, 0));
     DL_TRY(dl_kernel(S[0], &t2, t1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
     DL_TRY(dl_kernel(S[1], &u0, nullptr, k_dl_bu<WORDS>, gu, threads, p, g, 0, 0));
     DL_TRY(dl_kernel(S[1], &u1, u0, k_dl_bu_defer<WORDS>, gd, threads, p, g, 0, 0));
-    DL_TRY(dl_kernel(S[1], &u2, u1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
+    if (IBFS_DL_FUSED_BU)
+      DL_TRY(dl_kernel(S[1], &u2, u1, k_dl_bu_hubs<WORDS>, gh, threads, p, g, 0, 0));
+    else
+      DL_TRY(dl_kernel(S[1], &u2, u1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
   }
 #undef DL_TRY
   *out = top;
