@@ -98,6 +98,7 @@ _SIGS = [
     ("ibfs_graph_device_csr", C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
     ("ibfs_graph_close", C.c_int, [_P]),
     ("ibfs_groupby", C.c_int, [_P, _P, C.c_int64, _P]),
+    ("ibfs_groupby_device", C.c_int, [_P, _P, C.c_int64, _P, _P]),
     ("ibfs_groupby_csr", C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
     ("ibfs_read_sources", C.c_int, [C.c_char_p, _P, C.c_int64, _I64P]),
     ("ibfs_write_sources", C.c_int, [C.c_char_p, _P, C.c_int64]),
@@ -342,6 +343,13 @@ class Graph:
         out = np.zeros_like(src)
         _check(_lib().ibfs_groupby(self._h, _ptr(src), len(src), _ptr(out)), "ibfs_groupby")
         return out
+
+    def groupby_device(self, src_ptr: int, n: int, out_ptr: int, pos_ptr: int | None = None):
+        """GroupBy of n device int32 sources into out_ptr (and their input
+        positions into pos_ptr), on the graph's stream."""
+        _check(_lib().ibfs_groupby_device(self._h, C.c_void_p(src_ptr), n, C.c_void_p(out_ptr),
+                                          C.c_void_p(pos_ptr) if pos_ptr else None),
+               "ibfs_groupby_device")
 
     def teps(self, depth: np.ndarray) -> int:
         depth = np.ascontiguousarray(depth)

@@ -28,7 +28,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp",
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", f"-I{INCLUDE}",
              "-I/usr/local/cuda/include"]
 
-LIB_CU = ["engine.cu", "devloop.cu", "bytes_alg.cu", "server.cu", "noalloc.cu"]
+LIB_CU = ["engine.cu", "devloop.cu", "groupby_dev.cu", "bytes_alg.cu", "server.cu", "noalloc.cu"]
 LIB_CPP = ["host_graph.cpp", "autotune.cpp"]
 HEADERS = ["bfs_device.cuh", "internal.h", "launch_common.cuh"]
 

@@ -21,6 +21,7 @@
 //   --alpha A --beta B direction-switch parameters (with switch-level -1)
 //   --thresholds S,L   degree thresholds of the small/large queues (32,512)
 //   --groupby          reorder sources with GroupBy before batching
+//   --groupby-device   the same order, computed on the GPU
 //   --plain            host-driven level loop (default: persistent kernel)
 //   --device-loop      kernel per phase, level loop on the device (CUDA graph
 //                      conditional nodes)
@@ -39,7 +40,7 @@
 static void usage() {
   std::printf("Input: /path/to/exe /path/to/beg /path/to/csr concurrent-count switch-level "
               "bfs_count [--sources F] [--depth-out F] [--width W] [--alpha A] [--beta B] "
-              "[--thresholds S,L] [--groupby] [--plain] [--device-loop] [--batched] [--repeat K] [--device D] "
+              "[--thresholds S,L] [--groupby] [--groupby-device] [--plain] [--device-loop] [--batched] [--repeat K] [--device D] "
               "[--seed S] [--depth-bytes 1|2] [--vertex-major]\n");
 }
 
@@ -87,6 +88,7 @@ int main(int argc, char** argv) {
         return -1;
       }
     } else if (a == "--groupby") o.groupby = 1;
+    else if (a == "--groupby-device") o.groupby = 2;
     else if (a == "--plain") o.mode = IBFS_MODE_PLAIN;
     else if (a == "--device-loop") o.mode = IBFS_MODE_DEVICE_LOOP;
     else if (a == "--batched") batched = true;

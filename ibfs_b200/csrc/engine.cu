@@ -334,6 +334,8 @@ struct ibfs_graph {
   int64_t V = 0, E = 0, max_deg = 0;
   HostCsr h;
   DevBuf beg, col;
+  DevBuf gbhub;         // GroupBy's hub of every vertex (-1: not eligible), device GroupBy
+  DevBuf gbin, gbkeys;  // device GroupBy: caller-order sources, sort keys
   int64_t defer_cap = 16;  // bound on deferred bottom-up hub chunks per level
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
@@ -369,6 +371,7 @@ static ibfs_status check_opts(const ibfs_opts* o) {
     return IBFS_ERR_INVALID_ARG;
   if (o->alpha <= 0 || o->beta <= 0) return IBFS_ERR_INVALID_ARG;
   if (o->sml_shed < 1 || o->lrg_shed < o->sml_shed - 1) return IBFS_ERR_INVALID_ARG;
+  if (o->groupby < 0 || o->groupby > 2) return IBFS_ERR_INVALID_ARG;
   if (o->groups < 0 || o->ctas_per_sm < 0 || o->timeout_ms < 0 || o->max_levels < 0)
     return IBFS_ERR_INVALID_ARG;
   if (o->bu_thread_max < 0 || o->bu_thread_max > (1 << 20)) return IBFS_ERR_INVALID_ARG;
@@ -593,6 +596,36 @@ static ibfs_status upload_graph(ibfs_graph* g) {
                        cudaMemcpyHostToDevice, g->stream));
     CU(cudaStreamSynchronize(g->stream));
   }
+  // GroupBy's hub of every vertex (GroupBy.cuh:19-84): for degree <= 128,
+  // the first neighbour in the caller's order whose degree is > 128; -1 when
+  // there is none or the vertex is not eligible.  One int per vertex, so that
+  // a device GroupBy is a key per source and a sort.
+  {
+    std::vector<int32_t> hub;
+    try {
+      hub.assign((size_t)g->V, -1);
+    } catch (const std::bad_alloc&) {
+      return IBFS_ERR_OOM;
+    }
+    const int64_t* bg = g->h.beg.data();
+    const int32_t* cl = g->h.col.data();
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t v = 0; v < g->V; v++) {
+      if (bg[v + 1] - bg[v] > 128) continue;
+      for (int64_t e = bg[v]; e < bg[v + 1]; e++) {
+        const int32_t u = cl[e];
+        if (bg[u + 1] - bg[u] > 128) {
+          hub[(size_t)v] = u;
+          break;
+        }
+      }
+    }
+    if ((s = g->gbhub.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(g->V, 1))) != IBFS_OK)
+      return s;
+    CU(cudaMemcpyAsync(g->gbhub.p, hub.data(), sizeof(int32_t) * (size_t)g->V,
+                       cudaMemcpyHostToDevice, g->stream));
+    CU(cudaStreamSynchronize(g->stream));
+  }
   CU(cudaStreamSynchronize(g->stream));
   int64_t md = 0;
   for (int64_t v = 0; v < g->V; v++) md = std::max(md, g->h.beg[v + 1] - g->h.beg[v]);
@@ -618,6 +651,9 @@ static void destroy_graph(ibfs_graph* g) {
   for (auto& m : g->groups) m.release();
   g->beg.release();
   g->col.release();
+  g->gbhub.release();
+  g->gbin.release();
+  g->gbkeys.release();
   g->d_groups.release();
   g->d_src.release();
   g->d_outrow.release();
@@ -713,6 +749,25 @@ extern "C" ibfs_status ibfs_set_stream(ibfs_graph* g, void* cuda_stream) {
   std::lock_guard<std::mutex> lk(g->mu);
   g->stream = cuda_stream ? (cudaStream_t)cuda_stream : g->own_stream;
   g->gcache.release();
+  return IBFS_OK;
+}
+
+// GroupBy of device-resident sources on the graph's GPU (groupby_dev.cu):
+// the same order as ibfs_groupby, computed on the device.  Asynchronous on
+// the graph's stream; allocates its sort keys once per size class.
+extern "C" ibfs_status ibfs_groupby_device(ibfs_graph* g, const int32_t* src_dev, int64_t n,
+                                           int32_t* out_dev, int32_t* pos_dev) {
+  if (!g || n < 0 || (n > 0 && (!src_dev || !out_dev)) || n > INT32_MAX)
+    return IBFS_ERR_INVALID_ARG;
+  if (n == 0) return IBFS_OK;
+  if (src_dev == out_dev) return IBFS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g->mu);
+  CU(cudaSetDevice(g->device));
+  ibfs_status s;
+  if ((s = g->gbkeys.ensure_pow2(sizeof(unsigned long long) * groupby_dev_pad(n))) != IBFS_OK)
+    return s;
+  CU(groupby_dev_run(g->gbhub.as<int32_t>(), src_dev, n, g->gbkeys.as<unsigned long long>(),
+                     out_dev, pos_dev, g->stream));
   return IBFS_OK;
 }
 
@@ -894,13 +949,39 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     ord.assign(src, src + n);  // already batched by the caller (the server)
     row.assign(rows_in, rows_in + n);
   } else {
-    order_sources(g, src, n, o.groupby != 0, &ord, &row);
+    // groupby 2: the device regroups (groupby_dev.cu) after the upload
+    order_sources(g, src, n, o.groupby == 1, &ord, &row);
   }
+  const bool dev_gb = o.groupby == 2 && !rows_in;
   ibfs_status bs;
   if ((bs = g->h_src.ensure(sizeof(int32_t) * n)) != IBFS_OK) return bs;
   if ((bs = g->h_outrow.ensure(sizeof(int32_t) * n)) != IBFS_OK) return bs;
   if ((bs = g->d_src.ensure_pow2(sizeof(int32_t) * n)) != IBFS_OK) return bs;
   if ((bs = g->d_outrow.ensure_pow2(sizeof(int32_t) * n)) != IBFS_OK) return bs;
+  int64_t gb_launches = 0;
+  if (dev_gb) {
+    const int64_t npad = groupby_dev_pad(n);
+    if ((bs = g->gbin.ensure_pow2(sizeof(int32_t) * n)) != IBFS_OK) return bs;
+    if ((bs = g->gbkeys.ensure_pow2(sizeof(unsigned long long) * npad)) != IBFS_OK) return bs;
+    int lg = 0;
+    while ((1LL << lg) < npad) lg++;
+    gb_launches = 2 + (npad <= 4096 ? 1 : (int64_t)lg * (lg + 1) / 2);
+  }
+  // sources and output rows to the device: as ordered on the host, or in the
+  // caller's order and regrouped there
+  auto upload_sources = [&](cudaStream_t cs) -> ibfs_status {
+    if (dev_gb) {
+      CU(cudaMemcpyAsync(g->gbin.p, g->h_src.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, cs));
+      CU(groupby_dev_run(g->gbhub.as<int32_t>(), g->gbin.as<int32_t>(), n,
+                         g->gbkeys.as<unsigned long long>(), g->d_src.as<int32_t>(),
+                         g->d_outrow.as<int32_t>(), cs));
+    } else {
+      CU(cudaMemcpyAsync(g->d_src.p, g->h_src.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, cs));
+      CU(cudaMemcpyAsync(g->d_outrow.p, g->h_outrow.p, sizeof(int32_t) * n,
+                         cudaMemcpyHostToDevice, cs));
+    }
+    return IBFS_OK;
+  };
   if ((bs = g->d_brec.ensure_pow2(sizeof(BatchRec) * rp.nbatches)) != IBFS_OK) return bs;
   if ((bs = g->h_brec.ensure(sizeof(BatchRec) * rp.nbatches)) != IBFS_OK) return bs;
   if ((bs = g->d_lrec.ensure_pow2(sizeof(LevelRec) * (size_t)rp.nbatches * kLrecCap)) != IBFS_OK)
@@ -988,8 +1069,10 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   }
 
   auto enqueue = [&](cudaStream_t cs, bool capturing) -> ibfs_status {
-    CU(cudaMemcpyAsync(g->d_src.p, g->h_src.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, cs));
-    CU(cudaMemcpyAsync(g->d_outrow.p, g->h_outrow.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, cs));
+    {
+      const ibfs_status us = upload_sources(cs);
+      if (us != IBFS_OK) return us;
+    }
     CU(cudaMemcpyAsync(g->d_groups.p, hgb, sizeof(GroupBufs) * rp.G, cudaMemcpyHostToDevice, cs));
     for (int i = 0; i < rp.G; i++) CU(cudaMemsetAsync(hgb[i].ctl, 0, sizeof(Ctl), cs));
     CU(cudaMemsetAsync(g->d_brec.p, 0, sizeof(BatchRec) * rp.nbatches, cs));
@@ -1057,8 +1140,10 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     }
   } else if (devloop) {
     // ---- device-driven schedule: one graph launch runs every level ------
-    CU(cudaMemcpyAsync(g->d_src.p, g->h_src.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(g->d_outrow.p, g->h_outrow.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    {
+      const ibfs_status us = upload_sources(s);
+      if (us != IBFS_OK) return us;
+    }
     CU(cudaMemcpyAsync(g->d_groups.p, hgb, sizeof(GroupBufs) * rp.G, cudaMemcpyHostToDevice, s));
     Ctl* hctl = g->h_par.as<Ctl>();  // host staging of the G control blocks
     for (int i = 0; i < rp.G; i++) {
@@ -1108,8 +1193,10 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     if (rp.host_out) CU(cudaMemcpyAsync(depth_out, dout, out_bytes, cudaMemcpyDeviceToHost, s));
   } else {
     // ---- plain schedule -------------------------------------------------
-    CU(cudaMemcpyAsync(g->d_src.p, g->h_src.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(g->d_outrow.p, g->h_outrow.p, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    {
+      const ibfs_status us = upload_sources(s);
+      if (us != IBFS_OK) return us;
+    }
     CU(cudaMemcpyAsync(g->d_groups.p, hgb, sizeof(GroupBufs) * 1, cudaMemcpyHostToDevice, s));
     CU(cudaMemsetAsync(g->d_brec.p, 0, sizeof(BatchRec) * rp.nbatches, s));
     CU(cudaEventRecord(g->ev0, s));
@@ -1227,7 +1314,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
       launches = rp.G;
       for (int b = 0; b < rp.nbatches; b++) launches += 6 + 4LL * (br[b].td + br[b].bu);
     }
-    st->gpu_launches = launches;
+    st->gpu_launches = launches + gb_launches;
     st->device_ms = ms;
     st->levels_len = 0;
     if (st->levels && st->levels_cap > 0) {

@@ -89,7 +89,8 @@ typedef struct ibfs_opts {
     int32_t sml_shed;      /* degree < sml_shed: one thread per vertex (default 32) */
     int32_t lrg_shed;      /* degree > lrg_shed: CTA chunks (default 512)         */
     int32_t mode;          /* ibfs_mode (default IBFS_MODE_AUTO)                  */
-    int32_t groupby;       /* 1: reorder sources with GroupBy before batching     */
+    int32_t groupby;       /* 1: reorder sources with GroupBy before batching (on
+                              the host); 2: the same order computed on the GPU  */
     int32_t depth_bytes;   /* 1 (INFTY 255) or 2 (INFTY 65535); 0: 1, widened to 2
                               automatically when a level exceeds 254              */
     int32_t groups;        /* batches run concurrently (0: auto; device loop: 4)  */
@@ -177,6 +178,13 @@ ibfs_status ibfs_graph_close(ibfs_graph *g);
 /* GroupBy reorder (host, exact restatement of GroupBy.cuh:19-84). */
 ibfs_status ibfs_groupby(const ibfs_graph *g, const int32_t *src_host,
                          int64_t n, int32_t *out_host);
+/* GroupBy of device-resident sources on the graph's GPU: the order of
+   ibfs_groupby (GroupBy.cuh:19-84), from a per-vertex hub table built at
+   upload and a sort of n keys.  out_dev[k] = the k-th source of the order;
+   pos_dev (optional) = its index in src_dev.  Asynchronous on the graph's
+   stream (ibfs_set_stream); src_dev and out_dev must not overlap. */
+ibfs_status ibfs_groupby_device(ibfs_graph *g, const int32_t *src_dev, int64_t n,
+                                int32_t *out_dev, int32_t *pos_dev);
 /* GroupBy on host CSR arrays (no graph handle, no GPU). */
 ibfs_status ibfs_groupby_csr(const int64_t *beg_host, const int32_t *col_host,
                              int64_t V, const int32_t *src_host, int64_t n,

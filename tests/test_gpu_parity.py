@@ -139,6 +139,14 @@ def test_degree_thresholds(thr):
                   switch_level=1000)
 
 
+@pytest.mark.parametrize("but", [1, 8, 1000])
+def test_bottom_up_thread_limit(but):
+    beg, col, g = graph("rmat13")
+    src = ib.sample_sources(beg, col, 200, seed=10)
+    for mode in (ib.MODE_PERSISTENT, ib.MODE_DEVICE_LOOP):
+        run_and_check(beg, col, g, src, width=128, mode=mode, bu_thread_max=but)
+
+
 def test_edge_case_graph():
     # two components, an isolated vertex, a hub, a self loop and duplicates in
     # the edge list (cleaned by the CSR builder), a 3-vertex path
