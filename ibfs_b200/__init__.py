@@ -16,6 +16,7 @@ from .api import (  # noqa: F401
     Opts,
     Server,
     Stats,
+    convert_text,
     csr_from_edges,
     default_opts,
     exported_names,

@@ -99,6 +99,9 @@ _SIGS = [
     ("ibfs_graph_close", C.c_int, [_P]),
     ("ibfs_groupby", C.c_int, [_P, _P, C.c_int64, _P]),
     ("ibfs_groupby_device", C.c_int, [_P, _P, C.c_int64, _P, _P]),
+    ("ibfs_convert_text", C.c_int, [C.c_char_p, C.c_int32, C.c_int64, C.c_int32, C.c_char_p,
+                                    C.c_char_p, C.c_int32, C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_int64)]),
     ("ibfs_groupby_csr", C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
     ("ibfs_read_sources", C.c_int, [C.c_char_p, _P, C.c_int64, _I64P]),
     ("ibfs_write_sources", C.c_int, [C.c_char_p, _P, C.c_int64]),
@@ -260,6 +263,20 @@ def groupby_csr(beg: np.ndarray, col: np.ndarray, src: np.ndarray) -> np.ndarray
     _check(_lib().ibfs_groupby_csr(_ptr(beg), _ptr(col), len(beg) - 1, _ptr(src), len(src),
                                    _ptr(out)), "ibfs_groupby_csr")
     return out
+
+
+def convert_text(text_path: str, reverse: bool = True, skip_lines: int = 0, clean: bool = False,
+                 out_prefix: str | None = None, device: int = 0) -> tuple[str, str, int, int]:
+    """Edge-list text -> <prefix>_beg_pos.bin / <prefix>_csr.bin on the GPU
+    (tuple_text_to_bin.cpp:56-310; prefix defaults to the input path).
+    Returns (beg_path, csr_path, V, E)."""
+    pre = out_prefix or text_path
+    bp, cp = pre + "_beg_pos.bin", pre + "_csr.bin"
+    V, E = C.c_int64(), C.c_int64()
+    _check(_lib().ibfs_convert_text(text_path.encode(), 1 if reverse else 0, skip_lines,
+                                    1 if clean else 0, bp.encode(), cp.encode(), device,
+                                    C.byref(V), C.byref(E)), "ibfs_convert_text")
+    return bp, cp, V.value, E.value
 
 
 def read_src_v(path: str) -> np.ndarray:

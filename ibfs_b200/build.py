@@ -28,7 +28,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp",
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", f"-I{INCLUDE}",
              "-I/usr/local/cuda/include"]
 
-LIB_CU = ["engine.cu", "devloop.cu", "groupby_dev.cu", "bytes_alg.cu", "server.cu", "noalloc.cu"]
+LIB_CU = ["engine.cu", "devloop.cu", "groupby_dev.cu", "convert.cu", "bytes_alg.cu", "server.cu", "noalloc.cu"]
 LIB_CPP = ["host_graph.cpp", "autotune.cpp"]
 HEADERS = ["bfs_device.cuh", "internal.h", "launch_common.cuh"]
 
@@ -103,6 +103,12 @@ def build_cli(verbose: bool = False) -> str:
         return out
     if _newer(out, [src, lib, os.path.join(INCLUDE, "ibfs.h")]):
         _run(["g++", "-O2", "-std=c++17", f"-I{INCLUDE}", src, "-o", out, f"-L{PKG}", "-libfs",
+              f"-Wl,-rpath,$ORIGIN/.."])
+    # the edge-list converter's command line (tuple_text_to_bin)
+    csrc = os.path.join(CSRC, "convert_cli.cpp")
+    cout = os.path.join(out_dir, "tuple_text_to_bin")
+    if os.path.exists(csrc) and _newer(cout, [csrc, lib, os.path.join(INCLUDE, "ibfs.h")]):
+        _run(["g++", "-O2", "-std=c++17", f"-I{INCLUDE}", csrc, "-o", cout, f"-L{PKG}", "-libfs",
               f"-Wl,-rpath,$ORIGIN/.."])
     return out
 

@@ -314,6 +314,18 @@ ibfs_status ibfs_csr_from_edges(const int32_t *src, const int32_t *dst,
 /* Write the reference's binary CSR pair (uint64 little-endian). */
 ibfs_status ibfs_write_csr(const char *beg_path, const char *csr_path,
                            const int64_t *beg, const int32_t *col, int64_t V);
+
+/* Edge-list text -> binary CSR files on the GPU: the reference converter
+   tuple_text_to_bin.cpp:56-310 (whitespace-separated id pairs after
+   `skip_lines` header lines; ids shifted by the smallest id).  clean = 0:
+   the reference's CSR exactly (file order within every list, both
+   directions with `reverse`, duplicates and self loops kept); clean = 1:
+   symmetrised, self loops dropped, lists sorted and deduplicated.  Writes
+   beg_path / csr_path in the iBFS format; V_out / E_out optional.  An odd
+   number of tokens is IBFS_ERR_FORMAT. */
+ibfs_status ibfs_convert_text(const char *text_path, int32_t reverse, int64_t skip_lines,
+                              int32_t clean, const char *beg_path, const char *csr_path,
+                              int32_t device, int64_t *V_out, int64_t *E_out);
 /* Sample n distinct sources uniformly (seeded) among vertices with degree
    > 0 (component < 0) or inside the largest connected component
    (component >= 0). */

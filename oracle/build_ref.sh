@@ -1,6 +1,7 @@
 #!/usr/bin/env bash
-# Build oracle/_ref/ref_harness from the reference's own sources, where they
-# lie (REF, default /root/reference).  Outputs go to oracle/_ref/ only.  The
+# Build oracle/_ref/ref_harness and oracle/_ref/tuple_text_to_bin from the
+# reference's own sources, where they lie (REF, default /root/reference).
+# Outputs go to oracle/_ref/ only.  The
 # reference's GPU code targets sm_35 and does not compile for sm_100a; the
 # headers are compiled here for sm_52 only so that their host functions can
 # run on the CPU -- no kernel of theirs is ever launched.
@@ -13,6 +14,12 @@ if [ ! -f "$REF/graph.h" ]; then
   exit 0
 fi
 mkdir -p "$OUT"
+# the reference's edge-list converter, one standalone C++ file
+CONV="$REF/tuple_text_to_binary_csr/tuple_text_to_bin.cpp"
+if [ -f "$CONV" ] && ! [ "$OUT/tuple_text_to_bin" -nt "$CONV" ]; then
+  g++ -O2 -w "$CONV" -o "$OUT/tuple_text_to_bin"
+  echo "built $OUT/tuple_text_to_bin"
+fi
 if [ -x "$OUT/ref_harness" ] && [ "$OUT/ref_harness" -nt "$HERE/ref_harness.cu" ]; then
   echo "up to date"
   exit 0
