@@ -1070,70 +1070,66 @@ __device__ __forceinline__ void interleave4(const uint32_t (&x)[4], uint32_t (&y
            (spread8(x[2] >> (8 * q)) << 2) | (spread8(x[3] >> (8 * q)) << 3);
 }
 
-// Source-major, one-byte depths, NP planes known at compile time: lane =
-// VPL consecutive vertices (groups of 4 interleaved at a time), one VPL-byte
-// store per source row, so a warp writes 32*VPL contiguous bytes of a row
-// per store instruction.  4 measured best on B200 (R-MAT scale 24: output
-// pass 1.20 ms per batch at 4, 1.62 at 8, 1.79 at 16): the wider lanes need
-// more registers than the extra store width saves.
-#ifndef IBFS_OUT_VPL
-#define IBFS_OUT_VPL 4
-#endif
-template <int WORDS, int NP, int VPL>
+// In-register transpose of a 32 x 32 bit matrix, LSB-first: afterwards
+// bit r of A[j] is what bit j of A[r] was.  Five rounds of block swaps
+// (16, 8, 4, 2, 1), 16 masked delta swaps each.
+__device__ __forceinline__ void transpose32(uint32_t (&A)[32]) {
+#pragma unroll
+  for (int lv = 0; lv < 5; lv++) {
+    const int j = 16 >> lv;
+    const uint32_t m = lv == 0 ? 0x0000FFFFu : lv == 1 ? 0x00FF00FFu : lv == 2 ? 0x0F0F0F0Fu
+                     : lv == 3 ? 0x33333333u : 0x55555555u;
+#pragma unroll
+    for (int r = 0; r < 32; r++) {
+      if (r & j) continue;
+      const uint32_t t = ((A[r] >> j) ^ A[r + j]) & m;
+      A[r + j] ^= t;
+      A[r] ^= t << j;
+    }
+  }
+}
+
+// Source-major, one-byte depths, NP (<= 8) planes known at compile time:
+// lane = 4 consecutive vertices, one 4-byte store per source row.  The
+// depth byte of (vertex i, source s) has bit b = bit s of plane b of vertex
+// i, or is 0xFF when bit s of the final status is clear: the 32 words
+// A[8i + b] = plane_b(i) | ~status(i) (zero planes above NP) form a 32 x 32
+// bit matrix whose transpose is exactly the 32 output words, one per
+// source, byte i = vertex i -- about 5 instructions per output byte
+// instead of the 14 of nibble extraction per source and plane.
+template <int WORDS, int NP>
 __device__ void output_sm_u8(const Params& p, const GroupBufs& gb, const int32_t* rows, int n_b,
                              const Team& t) {
-  constexpr int NG = VPL / 4;
+  static_assert(NP <= 8, "one-byte depths use at most 8 planes");
   const int lane = t.lane;
-  for (long long base = t.warp * (32LL * VPL); base < p.V; base += t.nwarps * (32LL * VPL)) {
-    const long long v0 = base + (long long)VPL * lane;
-    const bool fullv = p.vec_sm >= VPL && v0 + VPL - 1 < p.V;
+  for (long long base = t.warp * 128; base < p.V; base += t.nwarps * 128) {
+    const long long v0 = base + 4 * lane;
+    const bool full4 = p.vec_sm >= 4 && v0 + 3 < p.V;
 #pragma unroll 1
     for (int k = 0; k < WORDS && k * 32 < n_b; k++) {
-      uint32_t ys[NG][4], yp[NP > 0 ? NP : 1][NG][4];
+      uint32_t A[32];
 #pragma unroll
-      for (int g = 0; g < NG; g++) {
-        uint32_t x[4];
-        const long long vg = v0 + 4 * g;
+      for (int i = 0; i < 4; i++) {
+        const bool in = v0 + i < p.V;
+        const uint32_t nst = in ? ~gb.last[(size_t)(v0 + i) * WORDS + k] : 0xFFFFFFFFu;
 #pragma unroll
-        for (int i = 0; i < 4; i++) x[i] = vg + i < p.V ? gb.last[(size_t)(vg + i) * WORDS + k] : 0u;
-        interleave4(x, ys[g]);
-#pragma unroll
-        for (int b = 0; b < NP; b++) {
-          const uint32_t* pl = gb.planes + (size_t)b * p.plane_stride;
-#pragma unroll
-          for (int i = 0; i < 4; i++) x[i] = vg + i < p.V ? pl[(size_t)(vg + i) * WORDS + k] : 0u;
-          interleave4(x, yp[b][g]);
+        for (int b = 0; b < 8; b++) {
+          uint32_t x = 0u;
+          if (b < NP && in) x = gb.planes[(size_t)b * p.plane_stride + (size_t)(v0 + i) * WORDS + k];
+          A[8 * i + b] = x | nst;
         }
       }
+      transpose32(A);
       const int js = min(32, n_b - k * 32);
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-#pragma unroll
-        for (int r = 0; r < 8; r++) {
-          const int j = q * 8 + r;
-          if (j < js) {
-            uint32_t w[NG];
-#pragma unroll
-            for (int g = 0; g < NG; g++) {
-              w[g] = nib_to_bytes(~(ys[g][q] >> (4 * r)) & 0xFu) * 0xFFu;
-#pragma unroll
-              for (int b = 0; b < NP; b++) w[g] |= nib_to_bytes((yp[b][g][q] >> (4 * r)) & 0xFu) << b;
-            }
-            uint8_t* row = p.out + (size_t)rows[k * 32 + j] * (size_t)p.V;
-            if (fullv) {
-              if constexpr (VPL == 16) {
-                *reinterpret_cast<uint4*>(row + v0) = make_uint4(w[0], w[1], w[2], w[3]);
-              } else if constexpr (VPL == 8) {
-                *reinterpret_cast<uint2*>(row + v0) = make_uint2(w[0], w[1]);
-              } else {
-                *reinterpret_cast<uint32_t*>(row + v0) = w[0];
-              }
-            } else {
-#pragma unroll
-              for (int g = 0; g < NG; g++)
-                for (int i = 0; i < 4; i++)
-                  if (v0 + 4 * g + i < p.V) row[v0 + 4 * g + i] = (uint8_t)(w[g] >> (8 * i));
-            }
+      for (int j = 0; j < 32; j++) {
+        if (j < js) {
+          uint8_t* row = p.out + (size_t)rows[k * 32 + j] * (size_t)p.V;
+          if (full4) {
+            *reinterpret_cast<uint32_t*>(row + v0) = A[j];
+          } else {
+            for (int i = 0; i < 4; i++)
+              if (v0 + i < p.V) row[v0 + i] = (uint8_t)(A[j] >> (8 * i));
           }
         }
       }
@@ -1199,31 +1195,28 @@ __device__ void output_generic(const Params& p, const GroupBufs& gb, uint8_t* de
   }
 }
 
-// VPL: vertices per lane of the source-major path when the rows allow
-// vector stores of that width (the persistent kernel, at 64 registers,
-// keeps 4).
-template <int WORDS, int NP, int VPL>
+template <int WORDS, int NP>
 __device__ __forceinline__ void output_u8(const Params& p, const GroupBufs& gb, uint8_t* depth_vm,
                                           const int32_t* rows, int n_b, const Team& t) {
-  if (p.layout == 0) {
-    if (p.vec_sm >= VPL) output_sm_u8<WORDS, NP, VPL>(p, gb, rows, n_b, t);
-    else output_sm_u8<WORDS, NP, 4>(p, gb, rows, n_b, t);
-  } else {
-    output_vm_u8<WORDS, NP>(p, gb, depth_vm, n_b, t);
-  }
+  if (p.layout == 0) output_sm_u8<WORDS, NP>(p, gb, rows, n_b, t);
+  else output_vm_u8<WORDS, NP>(p, gb, depth_vm, n_b, t);
 }
 
-template <int WORDS, int VPL = IBFS_OUT_VPL>
+template <int WORDS>
 __device__ void output_phase(const Params& p, const GroupBufs& gb, uint8_t* depth_vm,
                              const int32_t* rows, int n_b, int max_level, const Team& t) {
   const int P = planes_for(max_level);
   if (p.db == 1) {
     switch (P) {
-      case 0: output_u8<WORDS, 0, VPL>(p, gb, depth_vm, rows, n_b, t); return;
-      case 1: output_u8<WORDS, 1, VPL>(p, gb, depth_vm, rows, n_b, t); return;
-      case 2: output_u8<WORDS, 2, VPL>(p, gb, depth_vm, rows, n_b, t); return;
-      case 3: output_u8<WORDS, 3, VPL>(p, gb, depth_vm, rows, n_b, t); return;
-      case 4: output_u8<WORDS, 4, VPL>(p, gb, depth_vm, rows, n_b, t); return;
+      case 0: output_u8<WORDS, 0>(p, gb, depth_vm, rows, n_b, t); return;
+      case 1: output_u8<WORDS, 1>(p, gb, depth_vm, rows, n_b, t); return;
+      case 2: output_u8<WORDS, 2>(p, gb, depth_vm, rows, n_b, t); return;
+      case 3: output_u8<WORDS, 3>(p, gb, depth_vm, rows, n_b, t); return;
+      case 4: output_u8<WORDS, 4>(p, gb, depth_vm, rows, n_b, t); return;
+      case 5: output_u8<WORDS, 5>(p, gb, depth_vm, rows, n_b, t); return;
+      case 6: output_u8<WORDS, 6>(p, gb, depth_vm, rows, n_b, t); return;
+      case 7: output_u8<WORDS, 7>(p, gb, depth_vm, rows, n_b, t); return;
+      case 8: output_u8<WORDS, 8>(p, gb, depth_vm, rows, n_b, t); return;
       default: break;
     }
   }

@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(THREADS, MINB) persistent_kernel(Params p) {
       }
       return;
     }
-    output_phase<WORDS, 4>(p, gb, batch_depth(p, b), s_rows, n_b, s_maxl, t);
+    output_phase<WORDS>(p, gb, batch_depth(p, b), s_rows, n_b, s_maxl, t);
     if (lead && level + 1 < p.lrec_cap) {
       // one extra record per batch: dir 2 = the output pass
       LevelRec r;
