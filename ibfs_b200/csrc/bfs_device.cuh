@@ -795,13 +795,19 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
   const uint32_t* front = chg_at(gb, p, level - 1);
   uint32_t* out = chg_at(gb, p, level);
   const int lane = t.lane;
-  // FUSED counters (as inspect_phase)
-  unsigned long long f_mf = 0, f_cnt = 0, f_cdeg = 0, f_teps = 0;
-  uint32_t f_fm[WORDS], full[WORDS];
+  // FUSED counters (as inspect_phase); degree sums of one thread's vertices
+  // are below E < 2^31, so 32 bits hold them
+  uint32_t f_mf = 0, f_cnt = 0, f_cdeg = 0;
+  unsigned long long f_teps = 0;
+  uint32_t full[WORDS];
 #pragma unroll
-  for (int k = 0; k < WORDS; k++) {
-    f_fm[k] = 0;
-    full[k] = full_word(n_b, k);
+  for (int k = 0; k < WORDS; k++) full[k] = full_word(n_b, k);
+  // the OR of the level's new bits: per warp step a warp OR-reduction into
+  // shared memory (fewer live registers than a per-thread accumulator)
+  __shared__ uint32_t s_fm[kMaxWords];
+  if (FUSED) {
+    if (threadIdx.x < kMaxWords) s_fm[threadIdx.x] = 0u;
+    __syncthreads();
   }
   const bool first_plane = (level & (level - 1)) == 0;
   const int pb = __ffs(level) - 1;
@@ -920,12 +926,14 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
 #pragma unroll
     for (int k = 0; k < WORDS; k++) ch |= acc[k] != l[k];
     ch = ch && need;
+    uint32_t nb[WORDS];
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) nb[k] = 0u;
     if constexpr (!FUSED) {
       if (ch) st_status<WORDS>(gb.curr + (size_t)v * WORDS, acc);
     } else if (valid) {
       st_status<WORDS>(gb.curr + (size_t)v * WORDS, acc);  // every vertex: curr = new status
       const bool epi = ch && !deferred;  // deferred hubs: bu_hub_epilogue
-      uint32_t nb[WORDS];
       uint32_t pop = 0;
       bool comp = true;
 #pragma unroll
@@ -933,13 +941,12 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
         nb[k] = epi ? (acc[k] & ~l[k]) : 0u;
         pop += __popc(nb[k]);
         comp = comp && acc[k] == full[k];
-        f_fm[k] |= nb[k];
       }
       if (epi) {
-        const unsigned long long deg = (unsigned long long)(b1 - b0);
+        const uint32_t deg = (uint32_t)(b1 - b0);
         f_cnt += 1;
         f_mf += deg;
-        f_teps += deg * pop;
+        f_teps += (unsigned long long)deg * pop;
         if (comp) f_cdeg += deg;
         if (!depth_ok) range = true;
       }
@@ -962,6 +969,13 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
       }
       ch = epi;
     }
+    if constexpr (FUSED) {
+#pragma unroll
+      for (int k = 0; k < WORDS; k++) {
+        const uint32_t r = __reduce_or_sync(0xFFFFFFFFu, nb[k]);
+        if (lane == 0 && r) atomicOr(&s_fm[k], r);
+      }
+    }
     const uint32_t bal = __ballot_sync(0xFFFFFFFFu, ch);
     if (lane == 0 && bal) atomicOr(out + (base >> 5), bal);
   }
@@ -971,8 +985,8 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
     cta_add_u64(&par->mf, f_mf);
     cta_add_u64(&par->cdeg, f_cdeg);
     cta_add_u64(&par->teps, f_teps);
-#pragma unroll
-    for (int k = 0; k < WORDS; k++) cta_or_u32(&par->fmask[k], f_fm[k]);
+    __syncthreads();
+    if (threadIdx.x < WORDS && s_fm[threadIdx.x]) atomicOr(&par->fmask[threadIdx.x], s_fm[threadIdx.x]);
   }
 }
 
