@@ -96,6 +96,7 @@ _SIGS = [
     ("ibfs_csr_read", C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_P), C.POINTER(_P), _I64P, _I64P]),
     ("ibfs_graph_info", C.c_int, [_P, _I64P, _I64P, _I64P]),
     ("ibfs_graph_device_csr", C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
+    ("ibfs_graph_vertex_order", C.c_int, [_P, C.POINTER(_P)]),
     ("ibfs_graph_close", C.c_int, [_P]),
     ("ibfs_groupby", C.c_int, [_P, _P, C.c_int64, _P]),
     ("ibfs_groupby_device", C.c_int, [_P, _P, C.c_int64, _P, _P]),
@@ -351,6 +352,12 @@ class Graph:
         b, c = C.c_void_p(), C.c_void_p()
         _check(_lib().ibfs_graph_device_csr(self._h, C.byref(b), C.byref(c)), "device_csr")
         return b.value, c.value
+
+    def vertex_order(self) -> int:
+        """Device pointer of new_of_old[V] (caller id -> internal id)."""
+        m = C.c_void_p()
+        _check(_lib().ibfs_graph_vertex_order(self._h, C.byref(m)), "ibfs_graph_vertex_order")
+        return m.value
 
     def set_stream(self, stream_ptr: int | None) -> None:
         _check(_lib().ibfs_set_stream(self._h, C.c_void_p(stream_ptr or 0)), "ibfs_set_stream")

@@ -138,6 +138,8 @@ struct Params {
   int col_vec;      // col is 16-byte aligned and padded by 4 entries (vector reads)
   int hub_t;        // bottom-up: a warp scans at most hub_t neighbours of a vertex;
                     // a hub still missing bits defers the rest in chunks
+  const int32_t* vmap;  // caller id -> internal id of the resident graph (null:
+                        // identical); the output pass reads statuses through it
 };
 
 // Neighbours one thread of the bottom-up thread path has in flight per step
@@ -1125,11 +1127,13 @@ __device__ void output_sm_u8(const Params& p, const GroupBufs& gb, const int32_t
 #pragma unroll
       for (int i = 0; i < 4; i++) {
         const bool in = v0 + i < p.V;
-        const uint32_t nst = in ? ~gb.last[(size_t)(v0 + i) * WORDS + k] : 0xFFFFFFFFu;
+        // rows are in the caller's vertex order; statuses in the graph's
+        const size_t vi = in ? (size_t)(p.vmap ? p.vmap[v0 + i] : v0 + i) : 0;
+        const uint32_t nst = in ? ~gb.last[vi * WORDS + k] : 0xFFFFFFFFu;
 #pragma unroll
         for (int b = 0; b < 8; b++) {
           uint32_t x = 0u;
-          if (b < NP && in) x = gb.planes[(size_t)b * p.plane_stride + (size_t)(v0 + i) * WORDS + k];
+          if (b < NP && in) x = gb.planes[(size_t)b * p.plane_stride + vi * WORDS + k];
           A[8 * i + b] = x | nst;
         }
       }
@@ -1158,12 +1162,13 @@ __device__ void output_vm_u8(const Params& p, const GroupBufs& gb, uint8_t* dept
   const bool vec = p.vec_out && (n_b % 4 == 0);
   for (long long v = t.tid; v < p.V; v += t.nthreads) {
     uint8_t* row = depth_vm + (size_t)v * n_b;
+    const size_t vi = (size_t)(p.vmap ? p.vmap[v] : v);
 #pragma unroll 1
     for (int k = 0; k < WORDS && k * 32 < n_b; k++) {
-      const uint32_t st = gb.last[(size_t)v * WORDS + k];
+      const uint32_t st = gb.last[vi * WORDS + k];
       uint32_t pw[NP > 0 ? NP : 1];
 #pragma unroll
-      for (int b = 0; b < NP; b++) pw[b] = gb.planes[(size_t)b * p.plane_stride + (size_t)v * WORDS + k];
+      for (int b = 0; b < NP; b++) pw[b] = gb.planes[(size_t)b * p.plane_stride + vi * WORDS + k];
       const int js = min(32, n_b - k * 32);
 #pragma unroll
       for (int j4 = 0; j4 < 8; j4++) {
@@ -1188,16 +1193,17 @@ __device__ void output_generic(const Params& p, const GroupBufs& gb, uint8_t* de
                                const int32_t* rows, int n_b, int P, const Team& t) {
   const uint32_t inf = p.db == 1 ? 0xFFu : 0xFFFFu;
   for (long long v = t.tid; v < p.V; v += t.nthreads) {
+    const size_t vi = (size_t)(p.vmap ? p.vmap[v] : v);
 #pragma unroll 1
     for (int k = 0; k < WORDS && k * 32 < n_b; k++) {
-      const uint32_t st = gb.last[(size_t)v * WORDS + k];
+      const uint32_t st = gb.last[vi * WORDS + k];
       const int js = min(32, n_b - k * 32);
       for (int j = 0; j < js; j++) {
         uint32_t d = inf;
         if ((st >> j) & 1u) {
           d = 0;
           for (int b = 0; b < P; b++)
-            d |= ((gb.planes[(size_t)b * p.plane_stride + (size_t)v * WORDS + k] >> j) & 1u) << b;
+            d |= ((gb.planes[(size_t)b * p.plane_stride + vi * WORDS + k] >> j) & 1u) << b;
         }
         uint8_t* dst = p.layout == 0
                            ? p.out + ((size_t)rows[k * 32 + j] * (size_t)p.V + (size_t)v) * p.db

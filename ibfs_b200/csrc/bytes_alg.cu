@@ -23,6 +23,7 @@ extern "C" ibfs_status ibfs_graph_device_csr(const ibfs_graph* g, const int64_t*
                                              const int32_t** col);
 namespace ibfs {
 const int32_t* graph_host_col(const ibfs_graph* g);
+const int64_t* graph_host_beg(const ibfs_graph* g);
 }
 extern "C" ibfs_status ibfs_graph_info(const ibfs_graph* g, int64_t* V, int64_t* E,
                                        int64_t* max_degree);
@@ -127,11 +128,19 @@ extern "C" ibfs_status ibfs_bytes_alg(ibfs_graph* g, const void* depth_dev, int6
   ibfs_graph_device_csr(g, &beg, &col);
   ibfs_graph_info(g, &V, &E, nullptr);
   const int words = width / 32;
-  // the model scans neighbours in the caller's CSR order (the device copy is
-  // reordered hub-first), so upload that order for the measurement
+  // the model works on the caller's CSR (the device copy is in the graph's
+  // internal vertex order), so upload that for the measurement
   int32_t* col_in = nullptr;
+  int64_t* beg_in = nullptr;
+  if (cudaMalloc(&beg_in, sizeof(int64_t) * (size_t)(V + 1)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return IBFS_ERR_OOM;
+  }
+  cudaMemcpy(beg_in, graph_host_beg(g), sizeof(int64_t) * (size_t)(V + 1), cudaMemcpyHostToDevice);
+  beg = beg_in;
   if (E > 0) {
     if (cudaMalloc(&col_in, sizeof(int32_t) * (size_t)E) != cudaSuccess) {
+      cudaFree(beg_in);
       (void)cudaGetLastError();
       return IBFS_ERR_OOM;
     }
@@ -143,6 +152,7 @@ extern "C" ibfs_status ibfs_bytes_alg(ibfs_graph* g, const void* depth_dev, int6
   unsigned* maxl = nullptr;
   if (cudaMalloc(&mask, sizeof(uint32_t) * (size_t)V * words) != cudaSuccess) {
     cudaFree(col_in);
+    cudaFree(beg_in);
     (void)cudaGetLastError();
     return IBFS_ERR_OOM;
   }
@@ -151,6 +161,7 @@ extern "C" ibfs_status ibfs_bytes_alg(ibfs_graph* g, const void* depth_dev, int6
     cudaFree(mask);
     cudaFree(acc);
     cudaFree(col_in);
+    cudaFree(beg_in);
     (void)cudaGetLastError();
     return IBFS_ERR_OOM;
   }
@@ -176,6 +187,7 @@ extern "C" ibfs_status ibfs_bytes_alg(ibfs_graph* g, const void* depth_dev, int6
   cudaFree(acc);
   cudaFree(maxl);
   cudaFree(col_in);
+  cudaFree(beg_in);
   *bytes = total;
   return st;
 }

@@ -82,11 +82,11 @@ __global__ void k_gb_sort_step(unsigned long long* keys, int64_t npad, int64_t k
 
 __global__ void k_gb_gather(const unsigned long long* __restrict__ keys,
                             const int32_t* __restrict__ src, int64_t n, int32_t* ord,
-                            int32_t* pos) {
+                            int32_t* pos, const int32_t* __restrict__ idmap) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int32_t p = (int32_t)(keys[i] & 0xFFFFFFFFull);
-    ord[i] = src[p];
+    ord[i] = idmap ? idmap[src[p]] : src[p];
     if (pos) pos[i] = p;
   }
 }
@@ -98,10 +98,11 @@ int64_t groupby_dev_pad(int64_t n) {
 }
 
 // src, ord, pos (optional) and keys (groupby_dev_pad(n) entries) are device
-// arrays; ord must not alias src.  Asynchronous on `s`.
+// arrays; ord must not alias src.  idmap (optional) renames the ordered ids
+// (caller ids -> the graph's internal order).  Asynchronous on `s`.
 cudaError_t groupby_dev_run(const int32_t* gb_hub, const int32_t* src, int64_t n,
                             unsigned long long* keys, int32_t* ord, int32_t* pos,
-                            cudaStream_t s) {
+                            cudaStream_t s, const int32_t* idmap) {
   if (n <= 0) return cudaSuccess;
   const int64_t npad = groupby_dev_pad(n);
   const int threads = 256;
@@ -114,7 +115,7 @@ cudaError_t groupby_dev_run(const int32_t* gb_hub, const int32_t* src, int64_t n
       for (int64_t j = k >> 1; j > 0; j >>= 1)
         k_gb_sort_step<<<blocks, threads, 0, s>>>(keys, npad, k, j);
   }
-  k_gb_gather<<<blocks, threads, 0, s>>>(keys, src, n, ord, pos);
+  k_gb_gather<<<blocks, threads, 0, s>>>(keys, src, n, ord, pos, idmap);
   return cudaGetLastError();
 }
 

@@ -53,7 +53,7 @@ cudaError_t persistent_occupancy(int words, int threads, size_t smem, int* per_s
 int64_t groupby_dev_pad(int64_t n);
 cudaError_t groupby_dev_run(const int32_t* gb_hub, const int32_t* src, int64_t n,
                             unsigned long long* keys, int32_t* ord, int32_t* pos,
-                            cudaStream_t s);
+                            cudaStream_t s, const int32_t* idmap = nullptr);
 // devloop.cu: the device-loop CUDA graph of one run (not instantiated).
 cudaError_t build_device_loop_graph(const Params& p, int words, int G, int sms, int threads,
                                     cudaGraph_t* out);

@@ -169,9 +169,14 @@ ibfs_status ibfs_csr_read(const char *beg_path, const char *csr_path,
                           int64_t **beg, int32_t **col, int64_t *V, int64_t *E);
 ibfs_status ibfs_graph_info(const ibfs_graph *g, int64_t *V, int64_t *E,
                             int64_t *max_degree);
-/* Device pointers of the resident CSR (beg int64[V+1], col int32[E]). */
+/* Device pointers of the resident CSR (beg int64[V+1], col int32[E]), in
+   the graph's internal vertex order: vertices sorted by degree, highest
+   first (ties by id), every list ascending.  ibfs_graph_vertex_order gives
+   the renaming; every other entry point takes and returns caller ids. */
 ibfs_status ibfs_graph_device_csr(const ibfs_graph *g, const int64_t **beg,
                                   const int32_t **col);
+/* Device array new_of_old[V]: the internal id of every caller vertex id. */
+ibfs_status ibfs_graph_vertex_order(const ibfs_graph *g, const int32_t **new_of_old);
 ibfs_status ibfs_graph_close(ibfs_graph *g);
 
 /* ---- sources ----------------------------------------------------------- */

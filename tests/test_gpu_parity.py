@@ -261,3 +261,33 @@ def test_device_loop_replay_and_records():
             assert st["gpu_launches"] == (st["groups"] + 6 * st["n_batches"]
                                           + 4 * (st["td_levels"] + st["bu_levels"]))
     assert recs[ib.MODE_PERSISTENT] == recs[ib.MODE_DEVICE_LOOP]
+
+
+def test_internal_vertex_order():
+    """The device CSR is the caller's graph renamed by degree (highest first,
+    ties by id) with ascending lists; results stay in caller ids."""
+    import torch
+
+    beg, col, g = graph("rmat10")
+    V = len(beg) - 1
+    bp, cp = g.device_csr()
+    mp = g.vertex_order()
+    dbeg = torch.empty(V + 1, dtype=torch.int64, device="cuda")
+    dcol = torch.empty(len(col), dtype=torch.int32, device="cuda")
+    dmap = torch.empty(V, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    from cuda.bindings import runtime as rt
+
+    for dst, src_ptr, nbytes in ((dbeg, bp, 8 * (V + 1)), (dcol, cp, 4 * len(col)),
+                                 (dmap, mp, 4 * V)):
+        err, = rt.cudaMemcpy(dst.data_ptr(), src_ptr, nbytes,
+                             rt.cudaMemcpyKind.cudaMemcpyDeviceToDevice)
+        assert err == rt.cudaError_t.cudaSuccess
+    torch.cuda.synchronize()
+    nb, nc, nm = dbeg.cpu().numpy(), dcol.cpu().numpy(), dmap.cpu().numpy()
+    deg = np.diff(beg)
+    order = np.argsort(-deg, kind="stable")
+    assert np.array_equal(nm[order], np.arange(V))
+    for new in range(0, V, 37):
+        old = order[new]
+        assert np.array_equal(nc[nb[new]:nb[new + 1]], np.sort(nm[col[beg[old]:beg[old + 1]]]))
