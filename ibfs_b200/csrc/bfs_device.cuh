@@ -140,6 +140,9 @@ struct Params {
                     // a hub still missing bits defers the rest in chunks
   const int32_t* vmap;  // caller id -> internal id of the resident graph (null:
                         // identical); the output pass reads statuses through it
+  long long big_prefix; // bottom-up: vertices [0, big_prefix) take one warp each
+                        // (degree-ordered graphs: the vertices above the
+                        // thread-path limit; a multiple of 32; 0 otherwise)
 };
 
 // Neighbours one thread of the bottom-up thread path has in flight per step
@@ -814,7 +817,100 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
   const bool first_plane = (level & (level - 1)) == 0;
   const int pb = __ffs(level) - 1;
   bool range = false;
-  for (long long base = t.warp * 32; base < p.V; base += t.nwarps * 32) {
+  // The degree order puts every vertex above the thread-path limit into the
+  // prefix [0, p.big_prefix): one warp per vertex there, so that the hubs,
+  // which that order packs into a few warps, are spread over all of them.
+  for (long long v = t.warp; v < p.big_prefix; v += t.nwarps) {
+    uint32_t l[WORDS];
+    ld_status<WORDS>(gb.last + (size_t)v * WORDS, l);
+    const long long e0 = p.beg[v], e1 = p.beg[v + 1];
+    bool need = false;
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) need |= (fm[k] & ~l[k]) != 0u;
+    need = need && e1 > e0;  // uniform across the warp
+    uint32_t a[WORDS];
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) a[k] = l[k];
+    bool defer = false;
+    if (need) {
+      const long long e_lim = (e1 - e0 > p.hub_t) ? e0 + p.hub_t : e1;
+      bool miss = true;
+      for (long long e = e0; e < e_lim; e += 32) {
+        uint32_t x[WORDS];
+#pragma unroll
+        for (int k = 0; k < WORDS; k++) x[k] = 0;
+        if (e + lane < e_lim) {
+          const int32_t u = p.col[e + lane];
+          if (!p.bu_filter || ((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u))
+            ld_status<WORDS>(gb.last + (size_t)u * WORDS, x);
+        }
+        miss = false;
+#pragma unroll
+        for (int k = 0; k < WORDS; k++) {
+          a[k] |= __reduce_or_sync(0xFFFFFFFFu, x[k]);
+          miss |= (fm[k] & ~a[k]) != 0u;
+        }
+        if (!miss) break;
+      }
+      defer = miss && e_lim < e1;
+      if (defer && lane == 0) {
+        const int nch = (int)((e1 - e_lim + kHubChunk - 1) / kHubChunk);
+        const int base0 = atomicAdd(hq_cnt, nch);
+        for (int c = 0; c < nch; c++) gb.hq[base0 + c] = make_int2((int)v, c);
+      }
+    }
+    bool ch = false;
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) ch |= a[k] != l[k];
+    if (lane == 0) {
+      if constexpr (!FUSED) {
+        if (ch) {
+          st_status<WORDS>(gb.curr + (size_t)v * WORDS, a);
+          atomicOr(out + (v >> 5), 1u << (v & 31));
+        }
+      } else {
+        st_status<WORDS>(gb.curr + (size_t)v * WORDS, a);  // every vertex: curr = new status
+        const bool epi = ch && !defer;
+        uint32_t nb[WORDS];
+        uint32_t pop = 0;
+        bool comp = true;
+#pragma unroll
+        for (int k = 0; k < WORDS; k++) {
+          nb[k] = epi ? (a[k] & ~l[k]) : 0u;
+          pop += __popc(nb[k]);
+          comp = comp && a[k] == full[k];
+          if (nb[k]) atomicOr(&s_fm[k], nb[k]);
+        }
+        if (epi) {
+          const uint32_t deg = (uint32_t)(e1 - e0);
+          f_cnt += 1;
+          f_mf += deg;
+          f_teps += (unsigned long long)deg * pop;
+          if (comp) f_cdeg += deg;
+          if (!depth_ok) range = true;
+          atomicOr(out + (v >> 5), 1u << (v & 31));
+        }
+        uint32_t* q0 = gb.planes + (size_t)v * WORDS;
+        if (first_plane) {
+          st_status<WORDS>(q0 + (size_t)pb * p.plane_stride, nb);
+        } else if (epi && depth_ok) {
+          unsigned rest = (unsigned)level;
+          while (rest) {
+            const int b0p = __ffs(rest) - 1;
+            rest &= rest - 1;
+            uint32_t* qa = q0 + (size_t)b0p * p.plane_stride;
+            uint32_t xa[WORDS];
+            ld_status<WORDS>(qa, xa);
+#pragma unroll
+            for (int k = 0; k < WORDS; k++) xa[k] |= nb[k];
+            st_status<WORDS>(qa, xa);
+          }
+        }
+      }
+    }
+  }
+  const long long start = p.big_prefix;  // a multiple of 32
+  for (long long base = start + t.warp * 32; base < p.V; base += t.nwarps * 32) {
     const long long v = base + lane;
     const bool valid = v < p.V;
     uint32_t l[WORDS], acc[WORDS];
