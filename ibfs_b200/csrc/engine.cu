@@ -374,7 +374,7 @@ static ibfs_status check_opts(const ibfs_opts* o) {
     return IBFS_ERR_INVALID_ARG;
   if (o->alpha <= 0 || o->beta <= 0) return IBFS_ERR_INVALID_ARG;
   if (o->sml_shed < 1 || o->lrg_shed < o->sml_shed - 1) return IBFS_ERR_INVALID_ARG;
-  if (o->groupby < 0 || o->groupby > 2) return IBFS_ERR_INVALID_ARG;
+  if (o->groupby < 0 || o->groupby > 3) return IBFS_ERR_INVALID_ARG;
   if (o->groups < 0 || o->ctas_per_sm < 0 || o->timeout_ms < 0 || o->max_levels < 0)
     return IBFS_ERR_INVALID_ARG;
   if (o->bu_thread_max < 0 || o->bu_thread_max > (1 << 20)) return IBFS_ERR_INVALID_ARG;
@@ -833,15 +833,17 @@ extern "C" ibfs_status ibfs_teps(const ibfs_graph* g, const void* depth_host, in
 
 // Order sources (GroupBy or identity) and map each ordered position to the
 // caller's index.  Duplicated ids keep their order of appearance.
-static void order_sources(const ibfs_graph* g, const int32_t* src, int64_t n, bool groupby,
+// rule: 0 none, 1 GroupBy (GroupBy.cuh:19-84), 3 the largest-hub variant
+static void order_sources(const ibfs_graph* g, const int32_t* src, int64_t n, int rule,
                           std::vector<int32_t>* ord, std::vector<int32_t>* row) {
   ord->assign(src, src + n);
   row->resize((size_t)n);
-  if (!groupby) {
+  if (rule != 1 && rule != 3) {
     std::iota(row->begin(), row->end(), 0);
     return;
   }
-  groupby_host(g->h.beg.data(), g->h.col.data(), g->V, src, n, ord->data());
+  if (rule == 3) groupby_host_maxhub(g->h.beg.data(), g->h.col.data(), g->V, src, n, ord->data());
+  else groupby_host(g->h.beg.data(), g->h.col.data(), g->V, src, n, ord->data());
   // map ids back to positions (stable for duplicates)
   std::vector<std::pair<int32_t, int32_t>> pos((size_t)n);
   for (int64_t i = 0; i < n; i++) pos[i] = {src[i], (int32_t)i};
@@ -980,7 +982,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     row.assign(rows_in, rows_in + n);
   } else {
     // groupby 2: the device regroups (groupby_dev.cu) after the upload
-    order_sources(g, src, n, o.groupby == 1, &ord, &row);
+    order_sources(g, src, n, o.groupby == 2 ? 0 : o.groupby, &ord, &row);
   }
   const bool dev_gb = o.groupby == 2 && !rows_in;
   ibfs_status bs;

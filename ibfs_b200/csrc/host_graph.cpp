@@ -191,6 +191,44 @@ void groupby_host(const int64_t* beg, const int32_t* col, int64_t V,
   (void)V;
 }
 
+// A GroupBy variant (ibfs_opts.groupby = 3, not in the reference): the same
+// eligibility (degree <= 128 with a neighbour of degree > 128), but the hub
+// of a source is its HIGHEST-degree neighbour (ties: smaller id) instead of
+// the first one in CSR order, and the groups come largest hub first.  Sources
+// that share the biggest hubs then share batches whatever the CSR order.
+void groupby_host_maxhub(const int64_t* beg, const int32_t* col, int64_t V,
+                         const int32_t* src, int64_t n, int32_t* out) {
+  const int64_t kHub = 128;
+  std::vector<int32_t> hub_of((size_t)n, -1);
+  for (int64_t i = 0; i < n; i++) {
+    const int32_t s = src[i];
+    if (beg[s + 1] - beg[s] > kHub) continue;
+    int64_t best = kHub;
+    for (int64_t j = beg[s]; j < beg[s + 1]; j++) {
+      const int32_t h = col[j];
+      const int64_t d = beg[h + 1] - beg[h];
+      if (d > best || (d == best && d > kHub && h < hub_of[i])) {
+        best = d;
+        hub_of[i] = h;
+      }
+    }
+  }
+  std::vector<int64_t> idx;
+  idx.reserve((size_t)n);
+  for (int64_t i = 0; i < n; i++)
+    if (hub_of[i] >= 0) idx.push_back(i);
+  std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) {
+    const int32_t ha = hub_of[a], hb = hub_of[b];
+    const int64_t da = beg[ha + 1] - beg[ha], db = beg[hb + 1] - beg[hb];
+    return da != db ? da > db : ha < hb;
+  });
+  int64_t k = 0;
+  for (int64_t i : idx) out[k++] = src[i];
+  for (int64_t i = 0; i < n; i++)
+    if (hub_of[i] < 0) out[k++] = src[i];
+  (void)V;
+}
+
 }  // namespace ibfs
 
 using namespace ibfs;

@@ -40,6 +40,8 @@ ibfs_status validate_csr(const int64_t* beg, const int32_t* col, int64_t V,
                          int64_t E);
 void groupby_host(const int64_t* beg, const int32_t* col, int64_t V,
                   const int32_t* src, int64_t n, int32_t* out);
+void groupby_host_maxhub(const int64_t* beg, const int32_t* col, int64_t V,
+                         const int32_t* src, int64_t n, int32_t* out);
 
 }  // namespace ibfs
 

@@ -90,7 +90,9 @@ typedef struct ibfs_opts {
     int32_t lrg_shed;      /* degree > lrg_shed: CTA chunks (default 512)         */
     int32_t mode;          /* ibfs_mode (default IBFS_MODE_AUTO)                  */
     int32_t groupby;       /* 1: reorder sources with GroupBy before batching (on
-                              the host); 2: the same order computed on the GPU  */
+                              the host); 2: the same order computed on the GPU;
+                              3: a variant that groups by each source's
+                              highest-degree hub, largest hubs first          */
     int32_t depth_bytes;   /* 1 (INFTY 255) or 2 (INFTY 65535); 0: 1, widened to 2
                               automatically when a level exceeds 254              */
     int32_t groups;        /* batches run concurrently (0: auto; device loop: 4)  */

@@ -74,3 +74,18 @@ def test_run_with_device_groupby(mode, layout):
             assert np.array_equal(c.depth, d.depth)
     finally:
         g.close()
+
+
+def test_largest_hub_variant_same_depths():
+    """groupby = 3 only changes which sources share a batch: every source's
+    depths and the edge count are those of the reference GroupBy run."""
+    beg, col = ib.gen_rmat(12, 16, seed=8)
+    g = ib.Graph.from_csr(beg, col)
+    try:
+        src = ib.sample_sources(beg, col, 400, seed=9)
+        a = g.run(src, width=128, groupby=1)
+        b = g.run(src, width=128, groupby=3)
+        assert np.array_equal(a.depth, b.depth)
+        assert a.stats["traversed_edges"] == b.stats["traversed_edges"]
+    finally:
+        g.close()
