@@ -268,7 +268,7 @@ def run_ours(args, cfg):
     opts = ib.default_opts(width=args.width, concurrent=args.concurrent,
                            mode={"devloop": ib.MODE_DEVICE_LOOP, "persistent": ib.MODE_PERSISTENT,
                                  "plain": ib.MODE_PLAIN}[args.mode],
-                           groupby=0 if args.no_groupby else 1,
+                           groupby=0 if args.no_groupby else args.groupby_rule,
                            use_graph=0 if args.no_graph and args.mode == "persistent" else 1,
                            depth_bytes=1, groups=args.groups)
     n = len(src)
@@ -304,7 +304,8 @@ def run_ours(args, cfg):
     # ---- roofline: algorithmic bytes of one run (outside the timed region)
     bytes_alg = None
     if not args.no_roofline:
-        order = g.groupby(src) if not args.no_groupby else src
+        order = (src if args.no_groupby else
+                 g.groupby_maxhub(src) if args.groupby_rule == 3 else g.groupby(src))
         pos = {}
         rows = []
         idx_of = {}
@@ -417,7 +418,9 @@ def run_ours(args, cfg):
                                                 (args.mode == "persistent" and not args.no_graph)
                                                 else ""),
                        "groups_requested": args.groups,
-                       "groupby": not args.no_groupby, "parallelism": f"source-shard x{world}",
+                       "groupby": (False if args.no_groupby else
+                                   {1: "reference", 2: "reference (on the GPU)",
+                                    3: "largest-hub variant"}[args.groupby_rule]), "parallelism": f"source-shard x{world}",
                        "l2": (f"inputs larger than L2 (CSR {(8 * (V + 1) + 4 * len(col)) / 1e9:.2f} GB, "
                               f"status {2 * V * args.width / 8 / 1e6:.0f} MB per batch)"
                               if 8 * (V + 1) + 4 * len(col) > 126e6 else
@@ -500,6 +503,9 @@ def main():
     ap.add_argument("--mode", default="auto", choices=["auto", "devloop", "persistent", "plain"])
     ap.add_argument("--no-groupby", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
+    # 1: the reference's GroupBy (headline), 2: the same on the GPU, 3: the
+    # largest-hub variant (same depths, other batch composition)
+    ap.add_argument("--groupby-rule", type=int, default=1, choices=[1, 2, 3])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-roofline", action="store_true")

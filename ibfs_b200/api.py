@@ -100,6 +100,7 @@ _SIGS = [
     ("ibfs_graph_close", C.c_int, [_P]),
     ("ibfs_groupby", C.c_int, [_P, _P, C.c_int64, _P]),
     ("ibfs_groupby_device", C.c_int, [_P, _P, C.c_int64, _P, _P]),
+    ("ibfs_groupby_maxhub", C.c_int, [_P, _P, C.c_int64, _P]),
     ("ibfs_convert_text", C.c_int, [C.c_char_p, C.c_int32, C.c_int64, C.c_int32, C.c_char_p,
                                     C.c_char_p, C.c_int32, C.POINTER(C.c_int64),
                                     C.POINTER(C.c_int64)]),
@@ -366,6 +367,14 @@ class Graph:
         src = np.ascontiguousarray(src, np.int32)
         out = np.zeros_like(src)
         _check(_lib().ibfs_groupby(self._h, _ptr(src), len(src), _ptr(out)), "ibfs_groupby")
+        return out
+
+    def groupby_maxhub(self, src: np.ndarray) -> np.ndarray:
+        """The batch order of groupby = 3 (sources keyed by their highest-degree hub)."""
+        src = np.ascontiguousarray(src, np.int32)
+        out = np.zeros_like(src)
+        _check(_lib().ibfs_groupby_maxhub(self._h, _ptr(src), len(src), _ptr(out)),
+               "ibfs_groupby_maxhub")
         return out
 
     def groupby_device(self, src_ptr: int, n: int, out_ptr: int, pos_ptr: int | None = None):

@@ -810,6 +810,16 @@ extern "C" ibfs_status ibfs_groupby(const ibfs_graph* g, const int32_t* src_host
   return IBFS_OK;
 }
 
+// The batch order of ibfs_opts.groupby = 3 (largest-hub variant) on the host.
+extern "C" ibfs_status ibfs_groupby_maxhub(const ibfs_graph* g, const int32_t* src_host,
+                                           int64_t n, int32_t* out_host) {
+  if (!g || (!src_host && n > 0) || (!out_host && n > 0) || n < 0) return IBFS_ERR_INVALID_ARG;
+  for (int64_t i = 0; i < n; i++)
+    if (src_host[i] < 0 || src_host[i] >= g->V) return IBFS_ERR_RANGE;
+  groupby_host_maxhub(g->h.beg.data(), g->h.col.data(), g->V, src_host, n, out_host);
+  return IBFS_OK;
+}
+
 extern "C" ibfs_status ibfs_teps(const ibfs_graph* g, const void* depth_host, int64_t n,
                                  int32_t depth_bytes, int64_t* edges) {
   if (!g || !depth_host || !edges || n < 0 || (depth_bytes != 1 && depth_bytes != 2))

@@ -185,6 +185,10 @@ ibfs_status ibfs_graph_close(ibfs_graph *g);
 /* GroupBy reorder (host, exact restatement of GroupBy.cuh:19-84). */
 ibfs_status ibfs_groupby(const ibfs_graph *g, const int32_t *src_host,
                          int64_t n, int32_t *out_host);
+/* The batch order of ibfs_opts.groupby = 3 (no counterpart in the reference:
+   its GroupBy variant keyed by each source's highest-degree hub). */
+ibfs_status ibfs_groupby_maxhub(const ibfs_graph *g, const int32_t *src_host, int64_t n,
+                                int32_t *out_host);
 /* GroupBy of device-resident sources on the graph's GPU: the order of
    ibfs_groupby (GroupBy.cuh:19-84), from a per-vertex hub table built at
    upload and a sort of n keys.  out_dev[k] = the k-th source of the order;
