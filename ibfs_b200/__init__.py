@@ -25,6 +25,7 @@ from .api import (  # noqa: F401
     gen_rmat,
     graph_reader,
     groupby_csr,
+    groupby_csr_maxhub,
     lib_path,
     read_csr,
     read_src_v,

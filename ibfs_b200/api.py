@@ -105,6 +105,7 @@ _SIGS = [
                                     C.c_char_p, C.c_int32, C.POINTER(C.c_int64),
                                     C.POINTER(C.c_int64)]),
     ("ibfs_groupby_csr", C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
+    ("ibfs_groupby_csr_maxhub", C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
     ("ibfs_read_sources", C.c_int, [C.c_char_p, _P, C.c_int64, _I64P]),
     ("ibfs_write_sources", C.c_int, [C.c_char_p, _P, C.c_int64]),
     ("ibfs_opts_default", None, [C.POINTER(Opts)]),
@@ -279,6 +280,17 @@ def convert_text(text_path: str, reverse: bool = True, skip_lines: int = 0, clea
                                     1 if clean else 0, bp.encode(), cp.encode(), device,
                                     C.byref(V), C.byref(E)), "ibfs_convert_text")
     return bp, cp, V.value, E.value
+
+
+def groupby_csr_maxhub(beg: np.ndarray, col: np.ndarray, src: np.ndarray) -> np.ndarray:
+    """The largest-hub GroupBy variant (groupby = 3) on host CSR arrays."""
+    beg = np.ascontiguousarray(beg, np.int64)
+    col = np.ascontiguousarray(col, np.int32)
+    src = np.ascontiguousarray(src, np.int32)
+    out = np.zeros_like(src)
+    _check(_lib().ibfs_groupby_csr_maxhub(_ptr(beg), _ptr(col), len(beg) - 1, _ptr(src),
+                                          len(src), _ptr(out)), "ibfs_groupby_csr_maxhub")
+    return out
 
 
 def read_src_v(path: str) -> np.ndarray:

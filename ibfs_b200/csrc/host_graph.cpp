@@ -579,6 +579,17 @@ extern "C" ibfs_status ibfs_groupby_csr(const int64_t* beg, const int32_t* col, 
   return IBFS_OK;
 }
 
+// The largest-hub GroupBy variant (ibfs_opts.groupby = 3) on host arrays.
+extern "C" ibfs_status ibfs_groupby_csr_maxhub(const int64_t* beg, const int32_t* col, int64_t V,
+                                               const int32_t* src, int64_t n, int32_t* out) {
+  if (!beg || (!col && beg[V] > 0) || V <= 0 || n < 0 || (n > 0 && (!src || !out)))
+    return IBFS_ERR_INVALID_ARG;
+  for (int64_t i = 0; i < n; i++)
+    if (src[i] < 0 || src[i] >= V) return IBFS_ERR_RANGE;
+  groupby_host_maxhub(beg, col, V, src, n, out);
+  return IBFS_OK;
+}
+
 extern "C" void ibfs_free(void* p) { std::free(p); }
 
 extern "C" ibfs_status ibfs_teps(const ibfs_graph* g, const void* depth_host,

@@ -200,6 +200,11 @@ ibfs_status ibfs_groupby_device(ibfs_graph *g, const int32_t *src_dev, int64_t n
 ibfs_status ibfs_groupby_csr(const int64_t *beg_host, const int32_t *col_host,
                              int64_t V, const int32_t *src_host, int64_t n,
                              int32_t *out_host);
+/* The largest-hub variant (groupby = 3) on host CSR arrays; no counterpart
+   in the reference. */
+ibfs_status ibfs_groupby_csr_maxhub(const int64_t *beg_host, const int32_t *col_host,
+                                    int64_t V, const int32_t *src_host, int64_t n,
+                                    int32_t *out_host);
 /* read_src_v format: one decimal vertex id per line.  With ids == NULL only
    *n is set; otherwise up to cap ids are written. */
 ibfs_status ibfs_read_sources(const char *path, int32_t *ids, int64_t cap,

@@ -150,3 +150,33 @@ def test_csr_from_edges_rejects_bad_ids():
     with pytest.raises(ib.IbfsError) as ei:
         ib.csr_from_edges(np.array([0, 5]), np.array([1, 2]), 3)
     assert ei.value.status == 3
+
+
+
+def test_groupby_maxhub_variant_rule():
+    """The largest-hub GroupBy variant (groupby = 3) against a plain Python
+    statement of its rule: eligible sources (degree <= 128 with a neighbour
+    above 128) first, keyed by their highest-degree such neighbour (ties:
+    smaller id), largest hubs first and stable; the rest after, in input
+    order."""
+    beg, col = ib.gen_rmat(11, 16, seed=17)
+    deg = np.diff(beg)
+    rng = np.random.default_rng(3)
+    src = rng.integers(0, len(deg), 500).astype(np.int32)
+
+    def hub(s):
+        if deg[s] > 128:
+            return -1
+        best, h = 128, -1
+        for u in col[beg[s]:beg[s + 1]].tolist():
+            if deg[u] > best or (deg[u] == best and best > 128 and u < h):
+                best, h = deg[u], u
+        return h
+
+    hubs = [hub(s) for s in src.tolist()]
+    elig = sorted((i for i in range(len(src)) if hubs[i] >= 0),
+                  key=lambda i: (-deg[hubs[i]], hubs[i]))
+    ref = np.array([src[i] for i in elig] + [src[i] for i in range(len(src)) if hubs[i] < 0],
+                   np.int32)
+    assert len(elig) > 50
+    assert np.array_equal(ib.groupby_csr_maxhub(beg, col, src), ref)
