@@ -21,13 +21,17 @@
 #ifndef IBFS_DL_BU_MINB
 #define IBFS_DL_BU_MINB 3
 #endif
+// block size of the bottom-up kernel (the other phases run 512 threads)
+#ifndef IBFS_DL_BU_THREADS
+#define IBFS_DL_BU_THREADS 512
+#endif
 #ifndef IBFS_DL_INSPECT_MINB
 #define IBFS_DL_INSPECT_MINB 3
 #endif
 #if IBFS_DL_BU_MINB > 0
-#define DL_BU_BOUNDS __launch_bounds__(512, IBFS_DL_BU_MINB)
+#define DL_BU_BOUNDS __launch_bounds__(IBFS_DL_BU_THREADS, IBFS_DL_BU_MINB)
 #else
-#define DL_BU_BOUNDS __launch_bounds__(512)
+#define DL_BU_BOUNDS __launch_bounds__(IBFS_DL_BU_THREADS)
 #endif
 #if IBFS_DL_INSPECT_MINB > 0
 #define DL_INSPECT_BOUNDS __launch_bounds__(512, IBFS_DL_INSPECT_MINB)
@@ -323,7 +327,7 @@ static cudaError_t build_device_loop(const Params& p, int G, int sms, int thread
   const int gq = occ_grid((const void*)k_dl_qbuild<WORDS>, threads, sms);
   const int gh = occ_grid((const void*)k_dl_bu_hubs<WORDS>, threads, sms);
   const int gt = occ_grid((const void*)k_dl_td<WORDS>, threads, sms);
-  const int gu = occ_grid((const void*)k_dl_bu<WORDS>, threads, sms);
+  const int gu = occ_grid((const void*)k_dl_bu<WORDS>, IBFS_DL_BU_THREADS, sms);
   const int gd = occ_grid((const void*)k_dl_bu_defer<WORDS>, threads, sms);
   const int go = occ_grid((const void*)k_dl_output<WORDS>, threads, sms);
 #define DL_TRY(call)                   \
@@ -359,7 +363,7 @@ static cudaError_t build_device_loop(const Params& p, int G, int sms, int thread
     DL_TRY(dl_kernel(S[0], &t0, nullptr, k_dl_qbuild<WORDS>, gq, threads, p, g, 0, 0));
     DL_TRY(dl_kernel(S[0], &t1, t0, k_dl_td<WORDS>, gt, threads, p, g, 0, 0));
     DL_TRY(dl_kernel(S[0], &t2, t1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
-    DL_TRY(dl_kernel(S[1], &u0, nullptr, k_dl_bu<WORDS>, gu, threads, p, g, 0, 0));
+    DL_TRY(dl_kernel(S[1], &u0, nullptr, k_dl_bu<WORDS>, gu, IBFS_DL_BU_THREADS, p, g, 0, 0));
     DL_TRY(dl_kernel(S[1], &u1, u0, k_dl_bu_defer<WORDS>, gd, threads, p, g, 0, 0));
     if (IBFS_DL_FUSED_BU)
       DL_TRY(dl_kernel(S[1], &u2, u1, k_dl_bu_hubs<WORDS>, gh, threads, p, g, 0, 0));
