@@ -392,10 +392,10 @@ static size_t group_bytes(int64_t V, int64_t E, int words, int C, int db, int lr
   return b;
 }
 
-// Occupancy levels of the persistent kernel: (threads per CTA, CTAs per SM
-// the register budget is sized for).
+// Occupancy levels of the persistent kernel: threads per CTA; the CTAs per
+// SM its register budget is sized for are 2, 6, 8 and 1 (the template
+// arguments below).
 static const int kOccThreads[4] = {512, 256, 256, 512};
-static const int kOccMinB[4] = {2, 6, 8, 1};
 
 template <int WORDS>
 static const void* persistent_fn(int level) {
