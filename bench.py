@@ -84,54 +84,113 @@ def peaks():
     return 6650.0, "fallback"
 
 
-class ClockSampler:
-    """nvidia-smi sampled every 200 ms during the timed region."""
+_REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown", "nvmlClocksThrottleReasonHwSlowdown"),
+            ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown",
+             "nvmlClocksThrottleReasonHwThermalSlowdown"),
+            ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown",
+             "nvmlClocksThrottleReasonSwThermalSlowdown"),
+            ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap", "nvmlClocksThrottleReasonSwPowerCap"),
+            ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown",
+             "nvmlClocksThrottleReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, index: int):
+
+class ClockSampler:
+    """SM clock, power and clock-event reasons of the benchmarked GPU, sampled
+    through NVML every `period_s` (10 ms) on a background thread during the
+    timed region; nvidia-smi at 50 ms when NVML is not available.  The GPU is
+    found by the UUID of the CUDA device (CUDA_VISIBLE_DEVICES may renumber
+    devices), else by its index."""
+
+    def __init__(self, index: int, period_s: float = 0.01):
         self.index = index
-        self.rows = []
+        self.period = period_s
+        self.rows = []  # (sm_mhz, max_mhz, power_w, set of active reasons)
         self.proc = None
+        self.thread = None
+        self._stop = threading.Event()
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(
+                uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _nvml_loop(self, nv, h):
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        bits = [(nm, getattr(nv, a, None) or getattr(nv, b, 0)) for nm, a, b in _REASONS]
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not self._stop.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                r = int(get_reasons(h))
+                self.rows.append((sm, mx, pw, {nm for nm, b in bits if b and (r & b)}))
+            except Exception:
+                pass
+            self._stop.wait(self.period)
 
     def __enter__(self):
         try:
+            nv, h = self._nvml_handle()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+            self.source = f"NVML every {self.period * 1e3:.0f} ms"
+            return self
+        except Exception:
+            pass
+        try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={SMI_FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread = threading.Thread(target=self._smi_read, daemon=True)
             self.thread.start()
+            self.source = "nvidia-smi every 50 ms"
         except Exception:
             self.proc = None
         return self
 
-    def _read(self):
+    def _smi_read(self):
+        names = [r[0] for r in _REASONS[:4]]
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            r = [x.strip() for x in line.split(",")]
+            try:
+                act = {nm for i, nm in enumerate(names)
+                       if len(r) > 4 + i and r[4 + i].lower().startswith("active")}
+                self.rows.append((float(r[0]), float(r[1]), float(r[2]), act))
+            except (ValueError, IndexError):
+                continue
 
     def __exit__(self, *a):
+        self._stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
 
     def summary(self):
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
-            try:
-                sm.append(float(r[0]))
-                mx = max(mx, float(r[1]))
-            except (ValueError, IndexError):
-                continue
-            for i, nm in enumerate(names):
-                if len(r) > 4 + i and r[4 + i].lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "source": self.source}
+        sm = [r[0] for r in self.rows]
+        reasons = set().union(*[r[3] for r in self.rows])
+        return {"sm_mhz": statistics.median(sm), "sm_mhz_min": min(sm),
+                "sm_max_mhz": max(r[1] for r in self.rows),
+                "power_w_max": round(max(r[2] for r in self.rows), 1),
+                "reasons": sorted(reasons), "samples": len(sm), "source": self.source}
 
 
 def dist_setup(args):
@@ -179,8 +238,10 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_sample(beg, col, src, budget_s: float = 20.0):
-    """Time the oracle on all host cores over a bounded sample of sources."""
+def cpu_sample(beg, col, src, budget_s: float = 20.0, keep_depths: bool = False):
+    """Time the oracle on all host cores over a bounded sample of sources (the
+    first k of `src`).  Returns (GTEPS, threads, k, seconds, depths): the
+    oracle's [k][V] depths when keep_depths, else None."""
     import oracle
 
     threads = oracle.max_threads()
@@ -188,18 +249,36 @@ def cpu_sample(beg, col, src, budget_s: float = 20.0):
     k = min(k, len(src))
     # calibrate on one wave so that the sample ends near budget_s
     t0 = time.perf_counter()
-    d, _ = oracle.bfs(beg, col, src[:k], 1, threads)
+    d, _ = oracle.bfs_auto(beg, col, src[:k], threads) if keep_depths else \
+        oracle.bfs(beg, col, src[:k], 1, threads)
     dt = time.perf_counter() - t0
     edges = oracle.teps(beg, d)
     waves = max(1, min(int(budget_s / max(dt, 1e-3)), len(src) // k))
     if waves > 1:
         sub = src[:k * waves]
+        del d
         t0 = time.perf_counter()
-        d, _ = oracle.bfs(beg, col, sub, 1, threads)
+        d, _ = oracle.bfs_auto(beg, col, sub, threads) if keep_depths else \
+            oracle.bfs(beg, col, sub, 1, threads)
         dt = time.perf_counter() - t0
         edges = oracle.teps(beg, d)
         k = len(sub)
-    return edges / dt / 1e9, threads, k, dt
+    return edges / dt / 1e9, threads, k, dt, (d if keep_depths else None)
+
+
+def parity_vs_oracle(out, ref: np.ndarray) -> dict:
+    """Compare the first len(ref) depth rows of `out` (device tensor, caller
+    source order) with the oracle's rows, row by row on the host."""
+    bad_rows, bad_bytes = 0, 0
+    for i in range(ref.shape[0]):
+        got = out[i].cpu().numpy()
+        if got.dtype != ref.dtype:
+            got = got.view(ref.dtype) if got.nbytes == ref[i].nbytes else got
+        nb = int(np.count_nonzero(got != ref[i])) if got.shape == ref[i].shape else ref.shape[1]
+        bad_rows += nb > 0
+        bad_bytes += nb
+    return {"checked_sources": int(ref.shape[0]), "mismatches": int(bad_bytes),
+            "mismatched_sources": int(bad_rows), "against": "CPU oracle (restated queue BFS)"}
 
 
 def run_reference(args, cfg):
@@ -217,7 +296,7 @@ def run_reference(args, cfg):
         budget = max(1.0, min(10.0, 150.0 / max(1, args.warmup + args.steps)))
     vals = []
     for i in range(args.warmup + args.steps):
-        g, thr, k, dt = cpu_sample(beg, col, src, budget_s=budget)
+        g, thr, k, dt, _ = cpu_sample(beg, col, src, budget_s=budget)
         if i >= args.warmup:
             vals.append(g)
     v = statistics.median(vals)
@@ -403,12 +482,19 @@ def run_ours(args, cfg):
         del host
 
     # ---- CPU baseline (rank 0, N=1 only)
-    cpu = None
+    # ---- and the same oracle rows as the parity check of this run's depths
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
-        gcpu, thr, k, dt = cpu_sample(beg, col, src, budget_s=args.cpu_budget)
+        gcpu, thr, k, dt, ref = cpu_sample(beg, col, src, budget_s=args.cpu_budget,
+                                           keep_depths=True)
         cpu = {"value": round(gcpu, 4), "unit": "GTEPS", "cores": thr, "kind": "port",
                "sample": f"{k} of {n} sources, oracle BFS (restated sequential queue BFS, "
                          f"OpenMP over sources), {dt:.1f} s"}
+        parity = parity_vs_oracle(out, ref)
+        import oracle
+
+        parity["oracle_edges"] = int(oracle.teps(beg, ref))
+        del ref
 
     if rank == 0:
         line = {
@@ -434,6 +520,7 @@ def run_ours(args, cfg):
                        "groups": res.stats["groups"], "td_levels": res.stats["td_levels"],
                        "bu_levels": res.stats["bu_levels"]},
             "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "parity": parity,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -126,6 +126,7 @@ _SIGS = [
     ("ibfs_server_wait", C.c_int, [_P, C.c_uint64, C.c_int32, _P, C.c_uint32,
                                    C.POINTER(QueryInfo)]),
     ("ibfs_server_stats_get", C.c_int, [_P, C.POINTER(ServerStats)]),
+    ("ibfs_server_arena_rows", C.c_int64, [C.c_int64, C.c_int64, C.c_int32]),
     ("ibfs_server_destroy", C.c_int, [_P]),
     ("ibfs_gen_rmat", C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                 C.c_uint64, C.POINTER(_P), C.POINTER(_P), _I64P, _I64P]),
@@ -448,6 +449,9 @@ class Graph:
                                    flags, C.byref(st)), "ibfs_run")
             return RunResult(None, _stats_dict(st), _levels(recs, st))
         db = o.depth_bytes or 1
+        if out is not None and (not out.flags.c_contiguous or out.size != n * self.V):
+            raise ValueError(f"out must be a C-contiguous array of {n}*{self.V} depths, "
+                             f"got shape {out.shape}")
         while True:
             dt = np.uint8 if db == 1 else np.uint16
             if out is None or out.dtype != dt:

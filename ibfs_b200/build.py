@@ -128,7 +128,10 @@ def build_ref(verbose: bool = False) -> str | None:
     script = os.path.join(ROOT, "oracle", "build_ref.sh")
     if not os.path.exists(script):
         return None
-    r = subprocess.run(["bash", script], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    # where the reference sources are mounted in the build container
+    ref = os.environ.get("IBFS_REFERENCE_DIR", "/root/reference")
+    r = subprocess.run(["bash", script, ref], stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                       text=True)
     if verbose:
         print(r.stdout)
     out = os.path.join(ROOT, "oracle", "_ref", "ref_harness")

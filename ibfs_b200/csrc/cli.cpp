@@ -22,7 +22,9 @@
 //   --thresholds S,L   degree thresholds of the small/large queues (32,512)
 //   --groupby          reorder sources with GroupBy before batching
 //   --groupby-device   the same order, computed on the GPU
-//   --plain            host-driven level loop (default: persistent kernel)
+//   --plain            host-driven level loop (default: the library's AUTO
+//                      schedule -- the persistent kernel on small graphs,
+//                      the device loop on large ones)
 //   --device-loop      kernel per phase, level loop on the device (CUDA graph
 //                      conditional nodes)
 //   --batched          all batches in one launch (CUDA graph), one report

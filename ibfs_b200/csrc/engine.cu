@@ -485,8 +485,17 @@ static ibfs_status ensure_workspace(ibfs_graph* g, const RunPlan& rp, const ibfs
   return IBFS_OK;
 }
 
+// Key of a captured persistent run.  A captured graph holds raw addresses:
+// the kernel's Params (CSR, sources, rows, output, group table, records,
+// vertex map), every group's workspace (copied from the pinned group table
+// at replay), the pinned staging buffers its copies read and write, and the
+// device GroupBy's buffers.  Any run outside the graph path may grow (free
+// and reallocate) one of them, so all of them are part of the key: a moved
+// buffer means a new capture, never a replay into freed memory.
 static std::string make_key(const ibfs_graph* g, const int32_t* src, int64_t n, const ibfs_opts& o,
-                            void* out, int layout, uint32_t flags, const RunPlan& rp) {
+                            void* out, int layout, uint32_t flags, const RunPlan& rp,
+                            const Params& p, const GroupBufs* hgb, int G,
+                            const void* const* extra, int n_extra) {
   std::string k;
   k.append(reinterpret_cast<const char*>(&o), sizeof(o));
   k.append(reinterpret_cast<const char*>(&rp), sizeof(rp));
@@ -495,6 +504,9 @@ static std::string make_key(const ibfs_graph* g, const int32_t* src, int64_t n, 
   k.append(reinterpret_cast<const char*>(&flags), sizeof(flags));
   k.append(reinterpret_cast<const char*>(&n), sizeof(n));
   k.append(reinterpret_cast<const char*>(&g->stream), sizeof(g->stream));
+  k.append(reinterpret_cast<const char*>(&p), sizeof(p));
+  k.append(reinterpret_cast<const char*>(hgb), sizeof(GroupBufs) * (size_t)G);
+  k.append(reinterpret_cast<const char*>(extra), sizeof(void*) * (size_t)n_extra);
   if (!(flags & IBFS_OUT_DEVICE)) k.append(reinterpret_cast<const char*>(src), sizeof(int32_t) * n);
   return k;
 }
@@ -1132,7 +1144,11 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   std::string key;
   bool replay = false;
   if (use_graph) {
-    key = make_key(g, src, n, o, depth_out, layout, flags, rp);
+    const void* extra[] = {g->h_src.p,  g->h_outrow.p, g->h_par.p,  g->d_src.p,
+                           g->d_outrow.p, g->d_groups.p, g->d_brec.p, g->d_lrec.p,
+                           g->d_out.p,  g->gbin.p,     g->gbkeys.p, g->gbhub.p};
+    key = make_key(g, src, n, o, depth_out, layout, flags, rp, p, hgb, rp.G, extra,
+                   (int)(sizeof(extra) / sizeof(extra[0])));
     replay = g->gcache.exec && g->gcache.key == key;
   }
 

@@ -16,7 +16,6 @@
 // before each launch.  Calls whose work overlaps on the same GPU (two
 // streams, two host threads) race on the array: callers must serialise them.
 #include <cstring>
-#include <mutex>
 
 #include <cuda_runtime.h>
 
@@ -29,33 +28,26 @@ constexpr size_t kScratchBytes = 64ull << 20;  // the fixed maximum
 constexpr int kMaxBatches = 16;
 constexpr int kLrecCap = 64;
 constexpr int kMaxSources = kMaxBatches * 256;
-constexpr int kMaxDevices = 64;
 
 // The scratch.  In host code `g_scratch` is only a stand-in symbol: its
 // device address comes from cudaGetSymbolAddress (scratch_base below).
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-std::mutex g_mu;
-void* g_base[kMaxDevices] = {};
-
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Device address of g_scratch on the current device; looked up once per
-// device (the first call on a device does it, so that first call should
-// come before any stream capture).
-ibfs_status scratch_base(int dev, unsigned char** out) {
-  if (dev < 0 || dev >= kMaxDevices) return IBFS_ERR_UNSUPPORTED;
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_base[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-      (void)cudaGetLastError();
-      return IBFS_ERR_CUDA;
-    }
-    g_base[dev] = p;
+// Device address of g_scratch in the current device's context.  Looked up
+// on every call (a cheap runtime query next to the launch), so that a new
+// context -- after cudaDeviceReset, say -- never receives a stale address.
+// The first call on a device also loads this library's device code there,
+// so that first call should come before any stream capture.
+ibfs_status scratch_base(unsigned char** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+  if (e != cudaSuccess || p == nullptr) {
+    (void)cudaGetLastError();
+    return IBFS_ERR_CUDA;
   }
-  *out = static_cast<unsigned char*>(g_base[dev]);
+  *out = static_cast<unsigned char*>(p);
   return IBFS_OK;
 }
 
@@ -107,7 +99,7 @@ extern "C" ibfs_status ibfs_run_static_scratch(const int64_t* beg_dev, const int
   int dev = 0;
   NA_CU(cudaGetDevice(&dev));
   unsigned char* base = nullptr;
-  ibfs_status st = scratch_base(dev, &base);
+  ibfs_status st = scratch_base(&base);
   if (st != IBFS_OK) return st;
   cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
 

@@ -223,6 +223,20 @@ static void worker_loop(ibfs_server* s) {
   }
 }
 
+// Rows of row_bytes that an arena of `bytes` holds, at most INT32_MAX: the
+// kernels receive output rows as int32 indices (row * V is computed in
+// 64 bits), so a larger count would wrap and write outside the arena.
+static int64_t server_arena_rows(size_t bytes, size_t row_bytes) {
+  if (row_bytes == 0) return 0;
+  const size_t r = bytes / row_bytes;
+  return r > (size_t)INT32_MAX ? (int64_t)INT32_MAX : (int64_t)r;
+}
+
+extern "C" int64_t ibfs_server_arena_rows(int64_t arena_bytes, int64_t V, int32_t depth_bytes) {
+  if (arena_bytes <= 0 || V <= 0 || (depth_bytes != 1 && depth_bytes != 2)) return 0;
+  return server_arena_rows((size_t)arena_bytes, (size_t)V * (size_t)depth_bytes);
+}
+
 extern "C" void ibfs_server_opts_default(ibfs_server_opts* o) {
   if (!o) return;
   std::memset(o, 0, sizeof(*o));
@@ -266,7 +280,8 @@ extern "C" ibfs_status ibfs_server_create(ibfs_graph* g, const ibfs_server_opts*
     bytes = fr / 4;
   }
   const size_t row_bytes = (size_t)s->V * s->db;
-  const int64_t nrows = (int64_t)(bytes / row_bytes);
+  // rows travel to the kernel as int32 output-row indices
+  const int64_t nrows = server_arena_rows(bytes, row_bytes);
   if (nrows < 1) {
     delete s;
     return IBFS_ERR_OOM;
@@ -364,9 +379,18 @@ extern "C" ibfs_status ibfs_server_wait(ibfs_server* s, uint64_t qid, int32_t ti
   auto it = s->q.find(qid);
   if (it == s->q.end()) return IBFS_ERR_NOT_FOUND;
   const auto deadline = clock_t_::now() + std::chrono::milliseconds(timeout_ms);
-  while (!s->q[qid].done) {
-    if (s->cv.wait_until(lk, deadline) == std::cv_status::timeout && !s->q[qid].done)
-      return IBFS_ERR_TIMEOUT;
+  // look the query up afresh after every wake-up: another thread may have
+  // polled and collected it meanwhile
+  for (;;) {
+    it = s->q.find(qid);
+    if (it == s->q.end()) return IBFS_ERR_NOT_FOUND;
+    if (it->second.done) break;
+    if (s->cv.wait_until(lk, deadline) == std::cv_status::timeout) {
+      it = s->q.find(qid);
+      if (it == s->q.end()) return IBFS_ERR_NOT_FOUND;
+      if (!it->second.done) return IBFS_ERR_TIMEOUT;
+      break;
+    }
   }
   return collect_locked(s, qid, out, flags, info);
 }

@@ -265,6 +265,10 @@ ibfs_status ibfs_server_poll(ibfs_server *s, uint64_t qid, void *depth_out,
 ibfs_status ibfs_server_wait(ibfs_server *s, uint64_t qid, int32_t timeout_ms,
                              void *depth_out, uint32_t flags, ibfs_query_info *info);
 ibfs_status ibfs_server_stats_get(ibfs_server *s, ibfs_server_stats *out);
+/* Rows of V depths of depth_bytes each that an arena of arena_bytes holds:
+   the query capacity of ibfs_server_create, capped at INT32_MAX (output
+   rows are int32 indices on the device).  0 for invalid arguments. */
+int64_t ibfs_server_arena_rows(int64_t arena_bytes, int64_t V, int32_t depth_bytes);
 ibfs_status ibfs_server_destroy(ibfs_server *s);
 
 /* Per-graph tuning (no counterpart in the reference, whose constants are
@@ -301,8 +305,9 @@ ibfs_status ibfs_bytes_alg(ibfs_graph *g, const void *depth_dev, int64_t n,
    array inside the library (held by every GPU that loads it, until exit);
    graphs whose scratch does not fit, more than 16 batches, or a level past
    254 return IBFS_ERR_RANGE.  Runs on the calling thread's current device;
-   the first call on a device looks up the array's address, so make that
-   first call before any stream capture.  Calls share the array: calls whose
+   every call looks up the array's address in the current context, and the
+   first call on a device also loads the library's device code there, so
+   make that first call before any stream capture.  Calls share the array: calls whose
    work overlaps on one GPU race and must be serialised by the caller.
    Synchronises `cuda_stream` (a cudaStream_t, NULL = legacy stream) before
    returning; traversed_edges (may be NULL) receives the TEPS numerator. */

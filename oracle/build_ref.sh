@@ -1,13 +1,17 @@
 #!/usr/bin/env bash
 # Build oracle/_ref/ref_harness and oracle/_ref/tuple_text_to_bin from the
-# reference's own sources, where they lie (REF, default /root/reference).
-# Outputs go to oracle/_ref/ only.  The
+# reference's own sources, where they lie: the reference directory is the
+# first argument (or $REF).  Outputs go to oracle/_ref/ only.  The
 # reference's GPU code targets sm_35 and does not compile for sm_100a; the
 # headers are compiled here for sm_52 only so that their host functions can
 # run on the CPU -- no kernel of theirs is ever launched.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${REF:-/root/reference}"
+REF="${1:-${REF:-}}"
+if [ -z "$REF" ]; then
+  echo "usage: build_ref.sh <reference-dir> (or REF=<dir>)" >&2
+  exit 2
+fi
 OUT="$HERE/_ref"
 if [ ! -f "$REF/graph.h" ]; then
   echo "reference sources not present; keeping any prebuilt $OUT"

@@ -180,3 +180,16 @@ def test_groupby_maxhub_variant_rule():
                    np.int32)
     assert len(elig) > 50
     assert np.array_equal(ib.groupby_csr_maxhub(beg, col, src), ref)
+
+
+def test_server_arena_rows_clamped_to_int32():
+    """Output rows reach the kernels as int32 indices: the arena's row count
+    is capped at INT32_MAX however small the rows are."""
+    from ibfs_b200 import api
+
+    rows = api._lib().ibfs_server_arena_rows
+    assert rows(1000, 10, 1) == 100
+    assert rows(1000, 10, 2) == 50
+    assert rows(1 << 40, 1, 1) == 2**31 - 1
+    assert rows(1 << 34, 8, 2) == (1 << 34) // 16
+    assert rows(0, 10, 1) == 0 and rows(100, 0, 1) == 0 and rows(100, 10, 3) == 0

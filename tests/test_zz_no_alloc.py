@@ -4,10 +4,11 @@ It exists for callers that cannot call cudaMalloc: a plug-in inside a
 process whose own allocator owns the device memory, a latency-critical path
 that may not stall in an allocation, a deployment that forbids allocation
 after start-up.  Its scratch lives in a fixed device array inside the
-library, so these checks make sure that array is used correctly: two calls
-in a row (the second one smaller, so stale contents of the first would show)
-must give exactly the depths of the allocating entry point ibfs_run, and
-oversize requests must be refused with IBFS_ERR_RANGE rather than run.
+library, so these checks make sure that array is used correctly: calls in a
+row (later ones smaller, so stale contents of an earlier one would show), at
+every status width, must give exactly the depths of the allocating entry
+point ibfs_run and of the CPU oracle, and oversize requests must be refused
+with IBFS_ERR_RANGE rather than run.
 
 This file is collected last on purpose (test_zz_*): it must pass both alone
 in a fresh process and after every other test.
@@ -32,8 +33,19 @@ def _static_run(beg_d, col_d, V, E, src_d, n, width, out_d, stream):
     return st, edges.value
 
 
-def test_static_scratch_matches_ibfs_run_twice():
+def _source_major(flat: np.ndarray, n: int, V: int, width: int) -> np.ndarray:
+    """Vertex-major batches (batch b at b*V*width, rows of nb bytes) to [n][V]."""
+    rows = []
+    for b0 in range(0, n, width):
+        nb = min(width, n - b0)
+        rows.append(flat[b0 * V:b0 * V + V * nb].reshape(V, nb).T)
+    return np.concatenate(rows, axis=0)
+
+
+def test_static_scratch_matches_ibfs_run_and_oracle():
     import torch
+
+    import oracle
 
     beg, col = ib.gen_rmat(13, 16, seed=31)
     V, E = len(beg) - 1, len(col)
@@ -43,7 +55,10 @@ def test_static_scratch_matches_ibfs_run_twice():
     g = ib.Graph.from_csr(beg, col)
     stream = torch.cuda.current_stream(dev).cuda_stream
     try:
-        for call, (n, width, seed) in enumerate([(300, 128, 1), (70, 64, 2)]):
+        # calls in a row, each smaller than or different from the last, so that
+        # stale scratch contents of an earlier call would show; every width
+        calls = [(300, 128, 1), (70, 64, 2), (500, 256, 3), (45, 32, 4)]
+        for call, (n, width, seed) in enumerate(calls):
             src = ib.sample_sources(beg, col, n, seed=seed)
             src_d = torch.from_numpy(src).to(dev)
             out_static = torch.full((n * V,), 7, dtype=torch.uint8, device=dev)
@@ -57,6 +72,11 @@ def test_static_scratch_matches_ibfs_run_twice():
             a, b = out_static.cpu().numpy(), out_ref.cpu().numpy()
             assert np.array_equal(a, b), f"call {call}: {int((a != b).sum())} bytes differ"
             assert edges == res.stats["traversed_edges"]
+            # and directly against the CPU oracle
+            ref, _ = oracle.bfs(beg, col, src, 1)
+            got = _source_major(a, n, V, width)
+            assert np.array_equal(got, ref), f"call {call}: differs from the oracle"
+            assert edges == oracle.teps(beg, ref)
     finally:
         g.close()
 
