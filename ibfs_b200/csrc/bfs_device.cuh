@@ -154,6 +154,17 @@ constexpr int kBuStep = IBFS_BU_STEP;
 constexpr int kHubScan = 1024;   // neighbours one warp scans before deferring
 constexpr int kHubChunk = 2048;  // edges per deferred chunk (one CTA each)
 
+// Neighbour statuses of a bottom-up pass that runs as a kernel of its own
+// (RO: nothing writes `last` while it runs) are read through L1 (ld.global.nc):
+// most gathers hit the few hub words that the degree order packs into the
+// first lines of `last`, and L1 serves them instead of L2.  Measured on
+// R-MAT scale 24, one batch at a time: bottom-up 25.1 -> 19.4 ms per
+// 1024-source run; the persistent kernel, whose other phases write `last`
+// within the same launch, keeps L2 reads.
+#ifndef IBFS_BU_NC
+#define IBFS_BU_NC 1
+#endif
+
 // A team is the set of threads that share one batch: the whole grid in the
 // plain schedule, the CTAs of one group in the persistent kernel.
 struct Team {
@@ -199,6 +210,26 @@ __device__ __forceinline__ void st_status(uint32_t* p, const uint32_t (&x)[WORDS
   } else {
     __stcg(reinterpret_cast<uint4*>(p), make_uint4(x[0], x[1], x[2], x[3]));
     __stcg(reinterpret_cast<uint4*>(p) + 1, make_uint4(x[4], x[5], x[6], x[7]));
+  }
+}
+
+// Status read through the non-coherent (L1) path: only for buffers that no
+// thread writes while the kernel runs (`last` during a fused bottom-up pass).
+template <int WORDS>
+__device__ __forceinline__ void ld_status_nc(const uint32_t* p, uint32_t (&x)[WORDS]) {
+  if constexpr (WORDS == 1) {
+    x[0] = __ldg(p);
+  } else if constexpr (WORDS == 2) {
+    uint2 t = __ldg(reinterpret_cast<const uint2*>(p));
+    x[0] = t.x; x[1] = t.y;
+  } else if constexpr (WORDS == 4) {
+    uint4 t = __ldg(reinterpret_cast<const uint4*>(p));
+    x[0] = t.x; x[1] = t.y; x[2] = t.z; x[3] = t.w;
+  } else {
+    uint4 a = __ldg(reinterpret_cast<const uint4*>(p));
+    uint4 b = __ldg(reinterpret_cast<const uint4*>(p) + 1);
+    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+    x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
   }
 }
 
@@ -688,7 +719,7 @@ __device__ void td_phase(const Params& p, const GroupBufs& gb, int level, const 
 // other chunks of the same hub merge into with atomics, already covers
 // every frontier bit.  So one hub's long scan is spread over many CTAs
 // instead of holding one warp -- and the whole level -- for its adjacency.
-template <int WORDS>
+template <int WORDS, bool RO = false>
 __device__ void bu_defer_phase(const Params& p, const GroupBufs& gb, int level,
                                const uint32_t* fmask_g, const int32_t* hq_cnt, const Team& t) {
   __shared__ uint32_t s_acc[32][kMaxWords];
@@ -730,7 +761,8 @@ __device__ void bu_defer_phase(const Params& p, const GroupBufs& gb, int level,
       const int32_t u = p.col[e];
       if (p.bu_filter && !((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u)) continue;
       uint32_t x[WORDS];
-      ld_status<WORDS>(gb.last + (size_t)u * WORDS, x);
+      if constexpr (RO && IBFS_BU_NC) ld_status_nc<WORDS>(gb.last + (size_t)u * WORDS, x);
+      else ld_status<WORDS>(gb.last + (size_t)u * WORDS, x);
 #pragma unroll
       for (int k = 0; k < WORDS; k++) acc[k] |= x[k];
     }
@@ -790,10 +822,47 @@ __device__ void bu_defer_phase(const Params& p, const GroupBufs& gb, int level,
 // 2^b, so it needs no zeroing), and the changed bitmap is still marked for a
 // following top-down level.  Hubs deferred to bu_defer_phase get their
 // planes and counters in bu_hub_epilogue.
-template <int WORDS, bool FUSED = false>
+// Status of neighbour u for a bottom-up scan: from the CTA's shared-memory
+// copy of the hubs' statuses when u is one of the first hk vertices, else
+// from `last` (through L1 when NC: `last` is read-only during a fused pass).
+template <int WORDS, int HK, bool NC>
+__device__ __forceinline__ void ld_nbr(const uint32_t* last, const uint32_t* s_hub, long long hk,
+                                       int32_t u, uint32_t (&x)[WORDS]) {
+  if (HK > 0 && u < hk) {
+    if constexpr (WORDS >= 4) {
+#pragma unroll
+      for (int q = 0; q < WORDS / 4; q++) {
+        const uint4 t = reinterpret_cast<const uint4*>(s_hub + (size_t)u * WORDS)[q];
+        x[4 * q] = t.x; x[4 * q + 1] = t.y; x[4 * q + 2] = t.z; x[4 * q + 3] = t.w;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < WORDS; k++) x[k] = s_hub[(size_t)u * WORDS + k];
+    }
+    return;
+  }
+  if constexpr (NC) ld_status_nc<WORDS>(last + (size_t)u * WORDS, x);
+  else ld_status<WORDS>(last + (size_t)u * WORDS, x);
+}
+
+template <int WORDS, bool FUSED = false, bool RO = FUSED, int HK = 0>
 __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
                          const uint32_t* fmask_g, int32_t* hq_cnt, const Team& t,
                          Par* par = nullptr, int n_b = 0, bool depth_ok = true) {
+  constexpr bool NC = RO && IBFS_BU_NC;
+  // Hub status cache (HK > 0, passes that run as their own kernel: `last` is
+  // not written while they run).  The degree order puts the highest-degree vertices at
+  // internal ids 0..HK-1 and every adjacency list is ascending, so the first
+  // neighbours a scan reads -- the ones that usually complete it -- are these
+  // hubs: every CTA copies their previous-level statuses into shared memory
+  // once and reads them from there instead of from L2.
+  __shared__ __align__(16) uint32_t s_hub[HK > 0 ? HK * WORDS : 4];
+  long long hk = 0;
+  if constexpr (HK > 0) {
+    hk = min((long long)HK, (long long)p.V);
+    for (long long i = threadIdx.x; i < hk * WORDS; i += blockDim.x) s_hub[i] = __ldcg(gb.last + i);
+    __syncthreads();
+  }
   uint32_t fm[WORDS];
 #pragma unroll
   for (int k = 0; k < WORDS; k++) fm[k] = __ldcg(fmask_g + k);
@@ -842,7 +911,7 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
         if (e + lane < e_lim) {
           const int32_t u = p.col[e + lane];
           if (!p.bu_filter || ((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u))
-            ld_status<WORDS>(gb.last + (size_t)u * WORDS, x);
+            ld_nbr<WORDS, HK, NC>(gb.last, s_hub, hk, u, x);
         }
         miss = false;
 #pragma unroll
@@ -961,7 +1030,7 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
 #pragma unroll
         for (int i = 0; i < S; i++) {
           if (f[i]) {
-            ld_status<WORDS>(gb.last + (size_t)u[i] * WORDS, x[i]);
+            ld_nbr<WORDS, HK, NC>(gb.last, s_hub, hk, u[i], x[i]);
           } else {
 #pragma unroll
             for (int k = 0; k < WORDS; k++) x[i][k] = 0;
@@ -998,7 +1067,7 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
         if (e + lane < e_lim) {
           const int32_t u = p.col[e + lane];
           if (!p.bu_filter || ((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u))
-            ld_status<WORDS>(gb.last + (size_t)u * WORDS, x);
+            ld_nbr<WORDS, HK, NC>(gb.last, s_hub, hk, u, x);
         }
         miss = false;
 #pragma unroll

@@ -25,6 +25,14 @@
 #ifndef IBFS_DL_BU_THREADS
 #define IBFS_DL_BU_THREADS 512
 #endif
+// Shared memory per bottom-up CTA for the hubs' statuses (bytes; 0: off):
+// the first IBFS_BU_HUB_BYTES / (W/8) vertices of the degree order.  Off:
+// with the L1 path of IBFS_BU_NC the hub words already hit L1 (R-MAT scale
+// 24, one batch at a time, bottom-up per run: 19.4 ms L1 path, 20.0 ms with
+// a 32 KB cache, 20.1 ms with both).
+#ifndef IBFS_BU_HUB_BYTES
+#define IBFS_BU_HUB_BYTES 0
+#endif
 #ifndef IBFS_DL_INSPECT_MINB
 #define IBFS_DL_INSPECT_MINB 3
 #endif
@@ -201,13 +209,13 @@ __global__ void DL_BU_BOUNDS k_dl_bu(Params p, int g, CondH, CondH) {
   const int level = ls.level;
   const Team t = make_team(blockIdx.x, gridDim.x);
   if (IBFS_DL_FUSED_BU) {
-    bu_phase<WORDS, true>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
+    bu_phase<WORDS, true, true, IBFS_BU_HUB_BYTES / (4 * WORDS)>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
                           &gb.ctl->par[level & 1].hq_cnt, t, &gb.ctl->par[level & 1],
                           dl_batch_size(p, ls, ls.batch), level <= depth_limit(p.db));
   } else {
     zero_plane_if_first(p, gb, level, t);
-    bu_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
-                    &gb.ctl->par[level & 1].hq_cnt, t);
+    bu_phase<WORDS, false, true>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
+                                 &gb.ctl->par[level & 1].hq_cnt, t);
   }
 }
 
@@ -227,12 +235,21 @@ __global__ void __launch_bounds__(512) k_dl_bu_defer(Params p, int g, CondH, Con
   const GroupBufs gb = dl_bufs(p, g);
   const int level = gb.ctl->ls.level;
   if (gb.ctl->par[level & 1].hq_cnt == 0) return;  // uniform: nothing deferred
-  bu_defer_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
-                        &gb.ctl->par[level & 1].hq_cnt, make_team(blockIdx.x, gridDim.x));
+  bu_defer_phase<WORDS, true>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
+                              &gb.ctl->par[level & 1].hq_cnt, make_team(blockIdx.x, gridDim.x));
 }
 
+// threads per CTA and CTAs per SM of the output pass (R-MAT scale 24, one
+// batch at a time, output per 1024-source run: 512 x 1 10.6 ms, 512 x 2
+// (64 registers, spills) 15.9 ms, 256 x 3 17.0 ms)
+#ifndef IBFS_DL_OUT_THREADS
+#define IBFS_DL_OUT_THREADS 512
+#endif
+#ifndef IBFS_DL_OUT_MINB
+#define IBFS_DL_OUT_MINB 1
+#endif
 template <int WORDS>
-__global__ void __launch_bounds__(512) k_dl_output(Params p, int g, CondH, CondH) {
+__global__ void __launch_bounds__(IBFS_DL_OUT_THREADS, IBFS_DL_OUT_MINB) k_dl_output(Params p, int g, CondH, CondH) {
   __shared__ int32_t s_rows[kMaxWords * 32];
   const GroupBufs gb = dl_bufs(p, g);
   const LoopState& ls = gb.ctl->ls;
@@ -329,7 +346,7 @@ static cudaError_t build_device_loop(const Params& p, int G, int sms, int thread
   const int gt = occ_grid((const void*)k_dl_td<WORDS>, threads, sms);
   const int gu = occ_grid((const void*)k_dl_bu<WORDS>, IBFS_DL_BU_THREADS, sms);
   const int gd = occ_grid((const void*)k_dl_bu_defer<WORDS>, threads, sms);
-  const int go = occ_grid((const void*)k_dl_output<WORDS>, threads, sms);
+  const int go = occ_grid((const void*)k_dl_output<WORDS>, IBFS_DL_OUT_THREADS, sms);
 #define DL_TRY(call)                   \
   do {                                 \
     e = (call);                        \
@@ -352,7 +369,7 @@ static cudaError_t build_device_loop(const Params& p, int G, int sms, int thread
     DL_TRY(dl_kernel(B, &b2, b1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
     cudaGraph_t L = nullptr;
     DL_TRY(dl_cond(B, &b3, b2, hl, cudaGraphCondTypeWhile, 1, &L));
-    DL_TRY(dl_kernel(B, &b4, b3, k_dl_output<WORDS>, go, threads, p, g, 0, 0));
+    DL_TRY(dl_kernel(B, &b4, b3, k_dl_output<WORDS>, go, IBFS_DL_OUT_THREADS, p, g, 0, 0));
     DL_TRY(dl_kernel(B, &b5, b4, k_dl_batch_end, 1, 32, p, g, hb, 0));
     DL_TRY(cudaGraphConditionalHandleCreate(&hd, L, 2, cudaGraphCondAssignDefault));
     cudaGraphNode_t l0, l1;

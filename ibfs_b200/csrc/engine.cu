@@ -212,15 +212,15 @@ __global__ void __launch_bounds__(512) k_td(Params p, GroupBufs gb, int level) {
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_bu(Params p, GroupBufs gb, int level) {
   const Team t = make_team(blockIdx.x, gridDim.x);
-  bu_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
-                  &gb.ctl->par[level & 1].hq_cnt, t);
+  bu_phase<WORDS, false, true>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
+                               &gb.ctl->par[level & 1].hq_cnt, t);
 }
 
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_bu_defer(Params p, GroupBufs gb, int level) {
   const Team t = make_team(blockIdx.x, gridDim.x);
-  bu_defer_phase<WORDS>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
-                        &gb.ctl->par[level & 1].hq_cnt, t);
+  bu_defer_phase<WORDS, true>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
+                              &gb.ctl->par[level & 1].hq_cnt, t);
 }
 
 template <int WORDS>
