@@ -1253,7 +1253,8 @@ __device__ __forceinline__ void interleave4(const uint32_t (&x)[4], uint32_t (&y
 
 // In-register transpose of a 32 x 32 bit matrix, LSB-first: afterwards
 // bit r of A[j] is what bit j of A[r] was.  Five rounds of block swaps
-// (16, 8, 4, 2, 1), 16 masked delta swaps each.
+// (16, 8, 4, 2, 1), 16 masked delta swaps each; rows that are zero at
+// compile time fold away.
 __device__ __forceinline__ void transpose32(uint32_t (&A)[32]) {
 #pragma unroll
   for (int lv = 0; lv < 5; lv++) {
@@ -1274,10 +1275,12 @@ __device__ __forceinline__ void transpose32(uint32_t (&A)[32]) {
 // lane = 4 consecutive vertices, one 4-byte store per source row.  The
 // depth byte of (vertex i, source s) has bit b = bit s of plane b of vertex
 // i, or is 0xFF when bit s of the final status is clear: the 32 words
-// A[8i + b] = plane_b(i) | ~status(i) (zero planes above NP) form a 32 x 32
-// bit matrix whose transpose is exactly the 32 output words, one per
-// source, byte i = vertex i -- about 5 instructions per output byte
-// instead of the 14 of nibble extraction per source and plane.
+// A[8i + b] form a 32 x 32 bit matrix whose transpose is exactly the 32
+// output words, one per source, byte i = vertex i.  With NP <= 7 (depths
+// below 128) A[8i + b] = plane_b(i) for b < NP, 0 up to b = 6 and ~status(i)
+// for b = 7, and one sign-replicating byte permute per word turns bit 7
+// into 0xFF; the zero rows are compile-time constants that fold out of the
+// transpose.  With NP = 8, A[8i + b] = plane_b(i) | ~status(i).
 template <int WORDS, int NP>
 __device__ void output_sm_u8(const Params& p, const GroupBufs& gb, const int32_t* rows, int n_b,
                              const Team& t) {
@@ -1286,23 +1289,47 @@ __device__ void output_sm_u8(const Params& p, const GroupBufs& gb, const int32_t
   for (long long base = t.warp * 128; base < p.V; base += t.nwarps * 128) {
     const long long v0 = base + 4 * lane;
     const bool full4 = p.vec_sm >= 4 && v0 + 3 < p.V;
+    // rows are in the caller's vertex order; statuses in the graph's
+    uint32_t vis[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      vis[i] = v0 + i < p.V ? (uint32_t)(p.vmap ? p.vmap[v0 + i] : v0 + i) : 0u;
 #pragma unroll 1
     for (int k = 0; k < WORDS && k * 32 < n_b; k++) {
       uint32_t A[32];
 #pragma unroll
       for (int i = 0; i < 4; i++) {
         const bool in = v0 + i < p.V;
-        // rows are in the caller's vertex order; statuses in the graph's
-        const size_t vi = in ? (size_t)(p.vmap ? p.vmap[v0 + i] : v0 + i) : 0;
+        const size_t vi = vis[i];
         const uint32_t nst = in ? ~gb.last[vi * WORDS + k] : 0xFFFFFFFFu;
+        if constexpr (NP <= 7) {
+          // planes in rows 0..NP-1, zero rows up to 6 (folded away by the
+          // compiler), the unreached flag in row 7
 #pragma unroll
-        for (int b = 0; b < 8; b++) {
-          uint32_t x = 0u;
-          if (b < NP && in) x = gb.planes[(size_t)b * p.plane_stride + vi * WORDS + k];
-          A[8 * i + b] = x | nst;
+          for (int b = 0; b < 7; b++)
+            A[8 * i + b] = (b < NP && in) ? gb.planes[(size_t)b * p.plane_stride + vi * WORDS + k]
+                                          : 0u;
+          A[8 * i + 7] = nst;
+        } else {
+#pragma unroll
+          for (int b = 0; b < 8; b++) {
+            uint32_t x = 0u;
+            if (in) x = gb.planes[(size_t)b * p.plane_stride + vi * WORDS + k];
+            A[8 * i + b] = x | nst;
+          }
         }
       }
       transpose32(A);
+      if constexpr (NP <= 7) {
+        // byte i = depth (< 128) with bit 7 = unreached: widen bit 7 to the
+        // whole byte (prmt in sign-replicating mode), 0xFF = INFTY
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+          uint32_t m;
+          asm("prmt.b32 %0, %1, 0, 0xBA98;" : "=r"(m) : "r"(A[j]));
+          A[j] |= m;
+        }
+      }
       const int js = min(32, n_b - k * 32);
 #pragma unroll
       for (int j = 0; j < 32; j++) {
