@@ -29,7 +29,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", f"-I{INCLUDE}",
              "-I/usr/local/cuda/include"]
 
 LIB_CU = ["engine.cu", "devloop.cu", "groupby_dev.cu", "convert.cu", "bytes_alg.cu", "server.cu", "noalloc.cu"]
-LIB_CPP = ["host_graph.cpp", "autotune.cpp"]
+LIB_CPP = ["host_graph.cpp", "autotune.cpp", "sink.cpp"]
 HEADERS = ["bfs_device.cuh", "internal.h", "launch_common.cuh"]
 
 

@@ -143,6 +143,9 @@ struct Params {
   long long big_prefix; // bottom-up: vertices [0, big_prefix) take one warp each
                         // (degree-ordered graphs: the vertices above the
                         // thread-path limit; a multiple of 32; 0 otherwise)
+  int32_t* done_flags;  // per batch, in mapped host memory: 1 once the batch's
+                        // depths are complete in `out` (device loop), so that
+                        // the host can stream them out while later batches run
 };
 
 // Neighbours one thread of the bottom-up thread path has in flight per step

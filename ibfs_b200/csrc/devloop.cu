@@ -290,6 +290,12 @@ __global__ void k_dl_batch_end(Params p, int g, CondH h_batch, CondH) {
   r.err = 0;
   r.pad = 0;
   p.brec[b] = r;
+  if (p.done_flags) {
+    // the output kernel of batch b has finished (graph edge): tell the host,
+    // whose depth sink starts copying the batch's rows out
+    __threadfence_system();
+    *reinterpret_cast<volatile int32_t*>(p.done_flags + b) = 1;
+  }
   ls.batch = b + p.G;
   cudaGraphSetConditional(h_batch, ls.batch < ls.nbatches ? 1u : 0u);
 }

@@ -21,6 +21,7 @@
 #include <new>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -348,6 +349,13 @@ struct ibfs_graph {
   DevBuf d_groups, d_src, d_outrow, d_brec, d_lrec, d_out;
   PinBuf h_src, h_outrow, h_brec, h_lrec, h_par;
   GraphCache gcache;
+  // depth sink of host-buffer runs, and the device loop's per-batch done
+  // flags in mapped host memory (h_done; d_done is their device address)
+  DepthSink sink;
+  int32_t* h_done = nullptr;
+  int32_t* d_done = nullptr;
+  size_t done_cap = 0;
+  cudaEvent_t ev_out = nullptr;
   // device-loop graphs, keyed by the launch Params: a few entries, because a
   // server's rounds alternate between group counts (1..4 batches per round)
   static constexpr int kDlCache = 4;
@@ -574,6 +582,7 @@ static ibfs_status upload_graph(ibfs_graph* g) {
   g->stream = g->own_stream;
   CU(cudaEventCreate(&g->ev0));
   CU(cudaEventCreate(&g->ev1));
+  CU(cudaEventCreateWithFlags(&g->ev_out, cudaEventDisableTiming));
   // Internal vertex order: by degree, highest first (ties by caller id).
   // Vertices of similar degree then share warps (the bottom-up thread path
   // runs lanes of equal trip counts) and the hubs' status words, which most
@@ -701,6 +710,9 @@ static void destroy_graph(ibfs_graph* g) {
   g->h_brec.release();
   g->h_lrec.release();
   g->h_par.release();
+  g->sink.release();
+  if (g->h_done) cudaFreeHost(g->h_done);
+  if (g->ev_out) cudaEventDestroy(g->ev_out);
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
   if (g->own_stream) cudaStreamDestroy(g->own_stream);
@@ -1138,6 +1150,35 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   p.vec_sm = (g->V % 16 == 0 && (reinterpret_cast<uintptr_t>(dout) & 15) == 0)  ? 16
              : (g->V % 4 == 0 && (reinterpret_cast<uintptr_t>(dout) & 3) == 0) ? 4
                                                                               : 0;
+  // Per-batch done flags of the device loop, in mapped host memory, grown in
+  // powers of two so that their address (baked into cached graphs) stays put.
+  if ((size_t)rp.nbatches > g->done_cap) {
+    size_t cap = 64;
+    while (cap < (size_t)rp.nbatches) cap <<= 1;
+    if (g->h_done) cudaFreeHost(g->h_done);
+    g->h_done = nullptr;
+    g->d_done = nullptr;
+    g->done_cap = 0;
+    CU(cudaHostAlloc(reinterpret_cast<void**>(&g->h_done), cap * sizeof(int32_t),
+                     cudaHostAllocMapped));
+    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&g->d_done), g->h_done, 0));
+    g->done_cap = cap;
+  }
+  p.done_flags = g->d_done;
+  // The depth sink: a finished batch's rows (or its vertex-major block) go
+  // from `dout` to the caller's host buffer at the same byte offsets.
+  const int32_t* rows_host = g->h_outrow.as<int32_t>();
+  auto push_batch = [&](int b) -> cudaError_t {
+    const int64_t n_b = std::min<int64_t>(rp.C, n - (int64_t)b * rp.C);
+    const size_t rowb = (size_t)g->V * db;
+    if (layout == IBFS_LAYOUT_VERTEX_MAJOR)
+      return g->sink.push((size_t)b * rowb * rp.C, rowb * (size_t)n_b);
+    for (int64_t j = 0; j < n_b; j++) {
+      const cudaError_t e = g->sink.push((size_t)rows_host[(int64_t)b * rp.C + j] * rowb, rowb);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
 
   int64_t launches = 0;
   const bool use_graph = persistent && o.use_graph && !o.debug_withhold;
@@ -1271,10 +1312,44 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
       slot->exec = exec;
       slot->key = key;
     }
+    if (rp.host_out && dev_gb) {
+      // the device GroupBy chose the rows: the sink needs them on the host
+      CU(cudaMemcpyAsync(g->h_outrow.p, g->d_outrow.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost,
+                         s));
+      CU(cudaEventRecord(g->ev_out, s));
+    }
+    std::memset(g->h_done, 0, sizeof(int32_t) * (size_t)rp.nbatches);
     CU(cudaEventRecord(g->ev0, s));
     CU(cudaGraphLaunch(slot->exec, s));
     CU(cudaEventRecord(g->ev1, s));
-    if (rp.host_out) CU(cudaMemcpyAsync(depth_out, dout, out_bytes, cudaMemcpyDeviceToHost, s));
+    if (rp.host_out) {
+      // Stream every batch out as soon as its done flag is up, while the
+      // graph keeps traversing the others; batches whose flag never comes
+      // stopped on an error, which the records report below.
+      CU(g->sink.begin(g->device, depth_out, dout));
+      if (dev_gb) CU(cudaEventSynchronize(g->ev_out));
+      const volatile int32_t* fl = g->h_done;
+      std::vector<char> taken((size_t)rp.nbatches, 0);
+      int left = rp.nbatches;
+      bool graph_done = false;
+      while (left > 0) {
+        bool any = false;
+        for (int b = 0; b < rp.nbatches; b++) {
+          if (taken[(size_t)b] || fl[b] == 0) continue;
+          taken[(size_t)b] = 1;
+          left--;
+          any = true;
+          CU(push_batch(b));
+        }
+        if (left == 0 || any) continue;
+        if (graph_done) break;
+        const cudaError_t q = cudaEventQuery(g->ev1);
+        if (q == cudaSuccess) graph_done = true;  // one more scan, then stop
+        else if (q == cudaErrorNotReady) std::this_thread::sleep_for(std::chrono::microseconds(20));
+        else CU(q);
+      }
+      CU(g->sink.finish());
+    }
   } else {
     // ---- plain schedule -------------------------------------------------
     {
@@ -1291,6 +1366,14 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     LevelRec* hlr = g->h_lrec.as<LevelRec>();
     const size_t vpad = (size_t)((g->V + 31) & ~31LL);
     const size_t nchg = (size_t)(((g->V + 31) / 32 + 127) & ~127LL);
+    if (rp.host_out) {
+      CU(g->sink.begin(g->device, depth_out, dout));
+      if (dev_gb) {
+        CU(cudaMemcpyAsync(g->h_outrow.p, g->d_outrow.p, sizeof(int32_t) * n,
+                           cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+      }
+    }
     for (int b = 0; b < rp.nbatches; b++) {
       CU(cudaMemsetAsync(gb.last, 0, vpad * rp.words * 4, s));
       CU(cudaMemsetAsync(gb.curr, 0, vpad * rp.words * 4, s));
@@ -1341,13 +1424,20 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
       r.levels = level; r.max_level = max_level; r.td = td; r.bu = bu; r.teps = teps; r.err = err;
       if (err) {
         *range_hit = err == 3;
+        if (rp.host_out) (void)g->sink.finish();  // no copy may outlive the call
         return (ibfs_status)err;
       }
       CU(DISPATCH_WORDS(rp.words, launch_plain_output, p, gb, grid, thr, b, max_level, s));
       launches += 1;
+      if (rp.host_out) {
+        // the batch's rows go out on the sink's stream behind its output pass
+        CU(cudaEventRecord(g->ev_out, s));
+        CU(g->sink.wait_for(g->ev_out));
+        CU(push_batch(b));
+      }
     }
     CU(cudaEventRecord(g->ev1, s));
-    if (rp.host_out) CU(cudaMemcpyAsync(depth_out, dout, out_bytes, cudaMemcpyDeviceToHost, s));
+    if (rp.host_out) CU(g->sink.finish());
   }
   CU(cudaStreamSynchronize(s));
   // collect results

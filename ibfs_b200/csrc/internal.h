@@ -69,3 +69,48 @@ int graph_device(const ibfs_graph* g);
 const int64_t* graph_host_beg(const ibfs_graph* g);
 const int32_t* graph_host_col(const ibfs_graph* g);
 }  // namespace ibfs
+
+namespace ibfs {
+// sink.cpp: streams finished batches' depth rows (byte ranges of the device
+// output) to a host buffer on a copy stream of its own; pinned destinations
+// take direct copies, pageable ones a pinned staging ring.
+class DepthSink {
+ public:
+  ~DepthSink();
+  cudaError_t begin(int device, void* dst_host, const uint8_t* src_dev);
+  // the next copies wait for `ev` (recorded on the compute stream)
+  cudaError_t wait_for(cudaEvent_t ev);
+  // copy bytes [off, off + bytes) of the output to the same offset on the host
+  cudaError_t push(size_t off, size_t bytes);
+  // wait until every pushed range is in the host buffer
+  cudaError_t finish();
+  void release();
+  size_t copied() const { return copied_; }
+  bool pinned() const { return pinned_; }
+
+ private:
+  static constexpr int kSlots = 4;
+  static constexpr size_t kSlotBytes = 32u << 20;
+  struct Piece {
+    size_t off, at, bytes;  // output offset, offset in the slot, length
+  };
+  struct Slot {
+    void* buf = nullptr;
+    cudaEvent_t ev = nullptr;
+    std::vector<Piece> pieces;
+  };
+  cudaError_t drain_one();
+  cudaError_t close_open();
+  int device_ = -1;
+  cudaStream_t stream_ = nullptr;
+  std::vector<Slot> slots_;
+  std::vector<int> pending_;  // closed slots in copy order
+  int next_ = 0;
+  int open_ = -1;             // slot being filled (-1: none)
+  size_t fill_ = 0;
+  bool pinned_ = false;
+  uint8_t* dst_ = nullptr;
+  const uint8_t* src_ = nullptr;
+  size_t copied_ = 0;
+};
+}  // namespace ibfs
