@@ -364,6 +364,33 @@ def run_ours(args, cfg):
     for _ in range(max(args.warmup, 3)):
         res = step()
     stream.synchronize()
+    # The autotuner (coordinate descent over width, alpha/beta, queue
+    # thresholds and groups, each trial a real run) on a sample of the
+    # sources; the timed run then uses the options it picked, and the same
+    # run with the library defaults is timed beside it.  Every rank tunes on
+    # its own sample (deterministic per rank, no collective).
+    tuned = None
+    if args.tune:
+        t_tune = time.perf_counter()
+        base_opts = ib.Opts.from_buffer_copy(opts)
+        best, _, trials = g.autotune(src[:min(n, args.tune_sample)], base_opts, reps=2)
+        t_tune = time.perf_counter() - t_tune
+        ms_def = []
+        for _ in range(3):
+            ms_def.append(step().stats["device_ms"])
+        opts = ib.Opts.from_buffer_copy(best)
+        opts.use_graph = base_opts.use_graph
+        args.width = opts.width
+        args.concurrent = opts.concurrent
+        for _ in range(max(args.warmup, 3)):
+            res = step()
+        stream.synchronize()
+        tuned = {"sample_sources": int(min(n, args.tune_sample)), "trials": len(trials),
+                 "tune_s": round(t_tune, 2),
+                 "chosen": {"width": opts.width, "alpha": opts.alpha, "beta": opts.beta,
+                            "sml_shed": opts.sml_shed, "lrg_shed": opts.lrg_shed,
+                            "groups": opts.groups},
+                 "default_opts_ms_per_run": round(statistics.median(ms_def), 4)}
     barrier(world)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     kern_ms, launches, edges = [], 0, 0
@@ -518,7 +545,8 @@ def run_ours(args, cfg):
                               "inputs smaller than L2 (126 MB): warm-cache figure"),
                        "gen_s": round(t_gen, 1), "max_level": res.stats["max_level"],
                        "groups": res.stats["groups"], "td_levels": res.stats["td_levels"],
-                       "bu_levels": res.stats["bu_levels"]},
+                       "bu_levels": res.stats["bu_levels"],
+                       "tuned": tuned},
             "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "parity": parity,
             "clocks": clk.summary(),
@@ -541,25 +569,42 @@ def run_serving(args, cfg):
     from ibfs_b200 import serve_bench as sb
 
     torch.cuda.init()
+    t_gen = time.perf_counter()
     beg, col = make_graph(cfg)
+    t_gen = time.perf_counter() - t_gen
     g = ib.Graph.from_csr(beg, col)
     pool = ib.sample_sources(beg, col, 65536, seed=cfg["src_seed"])
     rates = [float(r) for r in args.rates.split(",")]
     sweep = []
-    for rate in rates:
-        nq = int(min(args.max_queries, max(200, rate * args.serve_seconds)))
-        qs, arr = sb.query_stream(pool, nq, rate, seed=int(rate))
-        served = sb.run_served(g, qs, arr, width=args.width, concurrent=args.concurrent,
-                               round_batches=args.round_batches, max_wait_us=args.max_wait_us,
-                               depth_bytes=1)
-        base = sb.run_one_per_launch(g, qs, arr, width=args.width)
-        sweep.append({"rate_qps": rate, "served": served, "one_query_per_launch": base})
+    kw = dict(width=args.width, concurrent=args.concurrent, round_batches=args.round_batches,
+              max_wait_us=args.max_wait_us, depth_bytes=1)
+    with ClockSampler(0) as clk:
+        for rate in rates:
+            nq = int(min(args.max_queries, max(200, rate * args.serve_seconds)))
+            qs, arr = sb.query_stream(pool, nq, rate, seed=int(rate))
+            served = sb.run_served(g, qs, arr, deliver=args.deliver, **kw)
+            base = sb.run_one_per_launch(g, qs, arr, width=args.width, budget_s=args.base_budget)
+            sweep.append({"rate_qps": rate, "served": served, "one_query_per_launch": base})
+            print(json.dumps({"rate_qps": rate, "served_p99_ms": round(served["p99_ms"], 2),
+                              "served_gteps": round(served["gteps"], 1),
+                              "base_p99_ms": round(base["p99_ms"], 2),
+                              "base_gteps": round(base["gteps"], 1)}), file=sys.stderr, flush=True)
+        # end to end through the public API with host buffers: every query's
+        # rows copied to pinned host memory, closed loop (all queries at once)
+        qs, _ = sb.query_stream(pool, args.e2e_queries, 1.0, seed=77)
+        e2e_run = sb.run_served(g, qs, np.zeros(len(qs)), deliver="host", **kw)
     # the headline point is the highest-throughput rate that meets the
     # latency objective (p99 <= --slo-p99-ms); beyond it latency is queueing,
     # reported apart as the saturated capacity
     ok = [x for x in sweep if x["served"]["p99_ms"] <= args.slo_p99_ms] or sweep[:1]
     top = max(ok, key=lambda x: x["served"]["gteps"])
     cap = max(sweep, key=lambda x: x["served"]["gteps"])
+    cpu = None
+    if not args.no_cpu:
+        src = ib.sample_sources(beg, col, 256, seed=cfg["src_seed"])
+        gcpu, thr, k, dt, _ = cpu_sample(beg, col, src, budget_s=args.cpu_budget)
+        cpu = {"value": round(gcpu, 4), "unit": "GTEPS", "cores": thr, "kind": "port",
+               "sample": f"{k} uniform sources, oracle BFS (OpenMP over sources), {dt:.1f} s"}
     line = {
         "metric": "aggregate GTEPS under Poisson load (served); p50/p99 query latency",
         "value": round(top["served"]["gteps"], 3), "unit": "GTEPS", "n_gpus": 1,
@@ -569,13 +614,28 @@ def run_serving(args, cfg):
         "config": {"workload": cfg["workload"], "V": int(len(beg) - 1), "E": int(len(col)),
                    "query_sources": "1-256 log-uniform", "width": args.width,
                    "round_batches": args.round_batches, "max_wait_us": args.max_wait_us,
-                   "latency": "submission to depths complete in HBM",
-                   "slo_p99_ms": args.slo_p99_ms},
+                   "latency": "submission to depths complete in HBM (the server's arena rows, "
+                              "collected by the client without a copy; the one-query-per-launch "
+                              "arm writes straight into the client's device buffer)"
+                              if args.deliver == "none" else
+                              f"submission to depths complete in HBM; delivered_* adds the copy "
+                              f"into the client's {args.deliver} buffer",
+                   "slo_p99_ms": args.slo_p99_ms, "gen_s": round(t_gen, 1)},
         "p50_ms": round(top["served"]["p50_ms"], 3), "p99_ms": round(top["served"]["p99_ms"], 3),
+        "delivered_p99_ms": round(top["served"]["delivered_p99_ms"], 3),
         "rate_qps": top["rate_qps"],
         "saturated": {"gteps": round(cap["served"]["gteps"], 3), "rate_qps": cap["rate_qps"],
                       "p50_ms": round(cap["served"]["p50_ms"], 3),
                       "p99_ms": round(cap["served"]["p99_ms"], 3)},
+        "e2e": {"value": round(e2e_run["gteps"], 3), "unit": "GTEPS",
+                "h2d_bytes_per_step": int(sum(4 * len(q) for q in qs)),
+                "d2h_bytes_per_step": int(sum(len(q) for q in qs) * (len(beg) - 1)),
+                "queries": len(qs), "p99_ms": round(e2e_run["delivered_p99_ms"], 3),
+                "how": "closed loop: all queries submitted at once, every query's rows copied "
+                       "to pinned host memory by ibfs_server_wait"},
+        "cpu_baseline": cpu,
+        "gpu_launches": int(sum(x["served"]["launches"] for x in sweep)),
+        "clocks": clk.summary(),
         "sweep": sweep,
     }
     print(json.dumps(line), flush=True)
@@ -598,20 +658,31 @@ def main():
     # 1: the reference's GroupBy (headline), 2: the same on the GPU, 3: the
     # largest-hub variant (same depths, other batch composition)
     ap.add_argument("--groupby-rule", type=int, default=1, choices=[1, 2, 3])
+    ap.add_argument("--tune", dest="tune", action="store_true", default=None,
+                    help="autotune on a sample before timing (default: on for c3, which "
+                         "is quoted autotuned)")
+    ap.add_argument("--no-tune", dest="tune", action="store_false")
+    ap.add_argument("--tune-sample", type=int, default=256)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-roofline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=None)
-    ap.add_argument("--rates", default="100,1000,2000,3000")
+    ap.add_argument("--rates", default="100,1000,2000,3000,5000,10000")
     ap.add_argument("--serve-seconds", type=float, default=3.0)
-    ap.add_argument("--max-queries", type=int, default=3000)
+    ap.add_argument("--max-queries", type=int, default=6000)
+    ap.add_argument("--base-budget", type=float, default=8.0)
+    ap.add_argument("--deliver", default="none", choices=["none", "device", "host"],
+                    help="where the served sweep's waiters copy each query's rows")
+    ap.add_argument("--e2e-queries", type=int, default=400)
     ap.add_argument("--round-batches", type=int, default=4)
     ap.add_argument("--slo-p99-ms", type=float, default=50.0)
     ap.add_argument("--max-wait-us", type=int, default=500)
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
+    if args.tune is None:
+        args.tune = args.config == "c3" and args.mode in ("auto", "devloop")
     if args.config == "c5" and args.impl != "reference":
         run_serving(args, cfg)
     elif args.impl == "reference":

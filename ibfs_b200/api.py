@@ -72,14 +72,14 @@ class ServerOpts(C.Structure):
 
 class QueryInfo(C.Structure):
     _fields_ = [("n_sources", C.c_int64), ("latency_ms", C.c_double), ("queue_ms", C.c_double),
-                ("status", C.c_int32), ("depth_bytes", C.c_int32)]
+                ("status", C.c_int32), ("depth_bytes", C.c_int32), ("delivered_ms", C.c_double)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("refused", C.c_int64),
                 ("rounds", C.c_int64), ("sources", C.c_int64), ("traversed_edges", C.c_int64),
                 ("busy_ms", C.c_double), ("wall_ms", C.c_double), ("arena_rows", C.c_int64),
-                ("arena_rows_used", C.c_int64)]
+                ("arena_rows_used", C.c_int64), ("launches", C.c_int64)]
 
 
 _LIB = None
@@ -539,12 +539,22 @@ class Server:
             return False, None, None
         return True, buf, _info(info)
 
-    def wait(self, qid: int, n: int, timeout_ms: int = 60000, want_depth: bool = True):
+    def wait(self, qid: int, n: int, timeout_ms: int = 60000, want_depth: bool = True,
+             out_ptr: int | None = None, on_device: bool = False):
+        """Block until the query is done and collect it: its depths into a new
+        array (want_depth), into caller memory at out_ptr (host, or device
+        with on_device; n*V*depth_bytes bytes), or nowhere."""
         info = QueryInfo()
-        buf = np.empty((n, self.V), np.uint8 if self.db == 1 else np.uint16) if want_depth \
-            else None
-        _check(_lib().ibfs_server_wait(self._h, qid, timeout_ms,
-                                       _ptr(buf) if buf is not None else None, 0, C.byref(info)),
+        if out_ptr is not None:
+            buf = None
+            dst = C.c_void_p(out_ptr)
+        else:
+            buf = np.empty((n, self.V), np.uint8 if self.db == 1 else np.uint16) if want_depth \
+                else None
+            dst = _ptr(buf) if buf is not None else None
+        _check(_lib().ibfs_server_wait(self._h, qid, timeout_ms, dst,
+                                       OUT_DEVICE if (on_device and out_ptr is not None) else 0,
+                                       C.byref(info)),
                "ibfs_server_wait")
         return buf, _info(info)
 

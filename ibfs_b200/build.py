@@ -28,9 +28,11 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp",
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", f"-I{INCLUDE}",
              "-I/usr/local/cuda/include"]
 
-LIB_CU = ["engine.cu", "devloop.cu", "groupby_dev.cu", "convert.cu", "bytes_alg.cu", "server.cu", "noalloc.cu"]
+LIB_CU = ["engine.cu", "persistent_w32.cu", "persistent_w64.cu", "persistent_w128.cu",
+          "persistent_w256.cu", "devloop.cu", "groupby_dev.cu", "convert.cu", "bytes_alg.cu",
+          "server.cu", "serve_loop.cu", "noalloc.cu"]
 LIB_CPP = ["host_graph.cpp", "autotune.cpp", "sink.cpp"]
-HEADERS = ["bfs_device.cuh", "internal.h", "launch_common.cuh"]
+HEADERS = ["bfs_device.cuh", "internal.h", "launch_common.cuh", "persistent.cuh"]
 
 
 def _nvcc() -> str:

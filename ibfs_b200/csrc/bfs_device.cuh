@@ -64,7 +64,7 @@ struct LoopState {
   int32_t err;
   int32_t flip;       // 1: the status "last" lives in GroupBufs::curr and vice versa
   int32_t sync;       // the next top-down level first copies new statuses over old ones
-  int32_t pad;
+  int32_t nb;         // sources of `batch`
   unsigned long long m_u, teps, prev_changed;
   unsigned long long t_lvl, t_mid;  // %globaltimer at the level start / inspect start
 };
@@ -146,6 +146,24 @@ struct Params {
   int32_t* done_flags;  // per batch, in mapped host memory: 1 once the batch's
                         // depths are complete in `out` (device loop), so that
                         // the host can stream them out while later batches run
+  // Serving queue (device loop, q_slots > 0): batches are not a fixed list
+  // but slots of a ring that the host fills while the graph runs.  The host
+  // writes a slot's sources (internal ids), output rows and count, then
+  // raises q_tail; a group that finishes a batch claims the next published
+  // one (q_head, compare-and-swap), copies the slot into src/out_row (device
+  // arrays of q_slots * C entries) and marks it 1 in q_state; after its
+  // output pass it writes brec[slot] and marks it 2.  A group that finds no
+  // published batch ends its batch loop; the host relaunches the graph for
+  // batches published after every group ended.
+  int q_slots;
+  const long long* q_tail;      // mapped host memory: batches published
+  const int32_t* q_n;           // mapped host memory [q_slots]: sources per slot
+  const int32_t* q_src;         // mapped host memory [q_slots * C]
+  const int32_t* q_rows;        // mapped host memory [q_slots * C]
+  int32_t* q_state;             // mapped host memory [q_slots]: 1 claimed, 2 done
+  unsigned long long* q_head;   // device memory: batches claimed
+  unsigned long long q_wait_ns; // a group that finds no published batch waits this
+                                // long for one (%globaltimer) before ending
 };
 
 // Neighbours one thread of the bottom-up thread path has in flight per step

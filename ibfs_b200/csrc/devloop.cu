@@ -61,9 +61,10 @@ namespace ibfs {
 using CondH = cudaGraphConditionalHandle;
 
 // The run's source and batch counts come from the control block, not from
-// Params, so that one built graph serves runs of any size.
-__device__ __forceinline__ int dl_batch_size(const Params& p, const LoopState& ls, int b) {
-  return (int)min((long long)p.C, ls.n_total - (long long)b * p.C);
+// Params, so that one built graph serves runs of any size; the batch loop
+// sets the size of every batch it starts (LoopState::nb).
+__device__ __forceinline__ int dl_batch_size(const Params&, const LoopState& ls, int) {
+  return ls.nb;
 }
 
 // Bottom-up levels run fused with their inspect work (bu_phase<.., true>):
@@ -83,13 +84,91 @@ __device__ __forceinline__ GroupBufs dl_bufs(const Params& p, int g) {
   return gb;
 }
 
+// ---- serving queue ---------------------------------------------------------
+__device__ __forceinline__ long long ld_acquire_sys_i64(const long long* p) {
+  long long v;
+  asm volatile("ld.acquire.sys.global.s64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Claim the next published batch of the serving queue (one thread).  Returns
+// its slot, or -1 when no batch was published within q_wait_ns (the group
+// then ends its batch loop; the host relaunches the graph for batches
+// published after every group ended).  Both waits are bounded: the empty
+// queue by q_wait_ns of %globaltimer, and lost compare-and-swaps (another
+// group took that batch) by kClaimTries.  The short wait keeps a group that
+// frees up between two publications alive instead of idle until the next
+// launch.
+constexpr int kClaimTries = 256;
+__device__ int serve_claim(const Params& p) {
+  const unsigned long long t0 = global_ns();
+  int lost = 0;
+  for (;;) {
+    const long long t = ld_acquire_sys_i64(p.q_tail);
+    const unsigned long long h = *reinterpret_cast<volatile unsigned long long*>(p.q_head);
+    if ((long long)h >= t) {
+      if (global_ns() - t0 >= p.q_wait_ns) return -1;
+      __nanosleep(1000);
+      continue;
+    }
+    if (atomicCAS(p.q_head, h, h + 1) == h) return (int)(h % (unsigned long long)p.q_slots);
+    if (++lost >= kClaimTries) return -1;
+  }
+}
+
+// Start the next batch of group g after `prev` (-1: the first).  Fixed runs
+// take batches g, g + G, ...; the serving queue takes the next published
+// slot and copies its sources and rows (host memory, read as volatile so
+// that no stale cached copy of an earlier use of the slot is seen) into the
+// device arrays that the phase kernels read.  Every thread of the block
+// calls this; thread 0 decides.  Returns whether a batch was started.
+__device__ bool dl_next_batch(const Params& p, Ctl* ctl, int g, int prev) {
+  __shared__ int s_b, s_n;
+  LoopState& ls = ctl->ls;
+  if (threadIdx.x == 0) {
+    int b = -1, nb = 0;
+    if (p.q_slots > 0) {
+      b = serve_claim(p);
+      if (b >= 0) {
+        nb = reinterpret_cast<const volatile int32_t*>(p.q_n)[b];
+        reinterpret_cast<volatile int32_t*>(p.q_state)[b] = 1;
+      }
+    } else {
+      b = prev < 0 ? g : prev + p.G;
+      if (b < ls.nbatches) nb = (int)min((long long)p.C, ls.n_total - (long long)b * p.C);
+      else b = -1;
+    }
+    s_b = b;
+    s_n = nb;
+  }
+  __syncthreads();
+  const int b = s_b, nb = s_n;
+  if (b >= 0 && p.q_slots > 0) {
+    const volatile int32_t* qs = p.q_src + (size_t)b * p.C;
+    const volatile int32_t* qr = p.q_rows + (size_t)b * p.C;
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+      const_cast<int32_t*>(p.src)[(size_t)b * p.C + j] = qs[j];
+      const_cast<int32_t*>(p.out_row)[(size_t)b * p.C + j] = qr[j];
+    }
+  }
+  if (threadIdx.x == 0 && b >= 0) {
+    ls.batch = b;
+    ls.nb = nb;
+  }
+  return b >= 0;
+}
+
+// Threads of the batch-loop kernels (k_dl_start, k_dl_batch_end): the
+// serving queue copies a slot's sources and rows with them.
+constexpr int kDlLoopThreads = 128;
+
 // First batch of group g; the batch loop runs while it exists.
 __global__ void k_dl_start(Params p, int g, CondH h_batch, CondH) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (blockIdx.x != 0) return;
   Ctl* ctl = p.groups[g].ctl;
-  ctl->ls.batch = g;
-  ctl->ls.err = 0;
-  cudaGraphSetConditional(h_batch, g < ctl->ls.nbatches ? 1u : 0u);
+  if (threadIdx.x == 0) ctl->ls.err = 0;
+  const bool go = dl_next_batch(p, ctl, g, -1);
+  if (threadIdx.x == 0) cudaGraphSetConditional(h_batch, go ? 1u : 0u);
 }
 
 // Zero the group's status words and bitmaps, reset the counters and the
@@ -260,19 +339,8 @@ __global__ void __launch_bounds__(IBFS_DL_OUT_THREADS, IBFS_DL_OUT_MINB) k_dl_ou
                       make_team(blockIdx.x, gridDim.x));
 }
 
-// End of a batch: its record (or the group's error), then the next batch of
-// the group; the batch loop ends after the last one or on an error.
-__global__ void k_dl_batch_end(Params p, int g, CondH h_batch, CondH) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  Ctl* ctl = p.groups[g].ctl;
-  LoopState& ls = ctl->ls;
-  const int b = ls.batch;
-  if (ls.err) {
-    atomicCAS(&ctl->err, 0, ls.err);
-    p.brec[b].err = ls.err;
-    cudaGraphSetConditional(h_batch, 0u);
-    return;
-  }
+// The records of a batch that finished without error (one thread).
+__device__ void dl_batch_record(const Params& p, LoopState& ls, int b) {
   if (ls.level + 1 < p.lrec_cap) {
     LevelRec r;  // dir 2: the batch's output pass
     r.batch = b; r.level = ls.level + 1; r.dir = 2; r.pad = 0;
@@ -296,8 +364,49 @@ __global__ void k_dl_batch_end(Params p, int g, CondH h_batch, CondH) {
     __threadfence_system();
     *reinterpret_cast<volatile int32_t*>(p.done_flags + b) = 1;
   }
-  ls.batch = b + p.G;
-  cudaGraphSetConditional(h_batch, ls.batch < ls.nbatches ? 1u : 0u);
+  if (p.q_slots > 0) {
+    // serving: the slot's depths are in their rows and its record (host
+    // memory) is written before the state says so
+    __threadfence_system();
+    reinterpret_cast<volatile int32_t*>(p.q_state)[b] = 2;
+  }
+}
+
+// End of a batch: its record (or the group's error), then the next batch of
+// the group; the batch loop ends after the last one or on an error (in the
+// serving queue: when no published batch is left; an error there is the
+// batch's own and goes into its record).
+__global__ void k_dl_batch_end(Params p, int g, CondH h_batch, CondH) {
+  if (blockIdx.x != 0) return;
+  Ctl* ctl = p.groups[g].ctl;
+  LoopState& ls = ctl->ls;
+  const int b = ls.batch;
+  __shared__ int s_stop;
+  if (threadIdx.x == 0) {
+    s_stop = 0;
+    if (ls.err && p.q_slots > 0) {
+      // serving: the error belongs to this batch's queries alone; report it
+      // in the slot's record and go on with the next batch
+      BatchRec r;
+      memset(&r, 0, sizeof(r));
+      r.err = ls.err;
+      p.brec[b] = r;
+      __threadfence_system();
+      reinterpret_cast<volatile int32_t*>(p.q_state)[b] = 2;
+      ls.err = 0;
+    } else if (ls.err) {
+      atomicCAS(&ctl->err, 0, ls.err);
+      p.brec[b].err = ls.err;
+      cudaGraphSetConditional(h_batch, 0u);
+      s_stop = 1;
+    } else {
+      dl_batch_record(p, ls, b);
+    }
+  }
+  __syncthreads();
+  if (s_stop) return;
+  const bool go = dl_next_batch(p, ctl, g, b);
+  if (threadIdx.x == 0) cudaGraphSetConditional(h_batch, go ? 1u : 0u);
 }
 
 // ---- device-driven schedule: graph construction ------------------------
@@ -365,7 +474,7 @@ static cudaError_t build_device_loop(const Params& p, int G, int sms, int thread
     CondH hb = 0, hl = 0, hd = 0;
     DL_TRY(cudaGraphConditionalHandleCreate(&hb, top, 0, cudaGraphCondAssignDefault));
     cudaGraphNode_t n0, n1;
-    DL_TRY(dl_kernel(top, &n0, nullptr, k_dl_start, 1, 32, p, g, hb, 0));
+    DL_TRY(dl_kernel(top, &n0, nullptr, k_dl_start, 1, kDlLoopThreads, p, g, hb, 0));
     cudaGraph_t B = nullptr;
     DL_TRY(dl_cond(top, &n1, n0, hb, cudaGraphCondTypeWhile, 1, &B));
     DL_TRY(cudaGraphConditionalHandleCreate(&hl, B, 0, cudaGraphCondAssignDefault));
@@ -376,7 +485,7 @@ static cudaError_t build_device_loop(const Params& p, int G, int sms, int thread
     cudaGraph_t L = nullptr;
     DL_TRY(dl_cond(B, &b3, b2, hl, cudaGraphCondTypeWhile, 1, &L));
     DL_TRY(dl_kernel(B, &b4, b3, k_dl_output<WORDS>, go, IBFS_DL_OUT_THREADS, p, g, 0, 0));
-    DL_TRY(dl_kernel(B, &b5, b4, k_dl_batch_end, 1, 32, p, g, hb, 0));
+    DL_TRY(dl_kernel(B, &b5, b4, k_dl_batch_end, 1, kDlLoopThreads, p, g, hb, 0));
     DL_TRY(cudaGraphConditionalHandleCreate(&hd, L, 2, cudaGraphCondAssignDefault));
     cudaGraphNode_t l0, l1;
     DL_TRY(dl_kernel(L, &l0, nullptr, k_dl_decide, 1, 32, p, g, hl, hd));

@@ -33,154 +33,9 @@
 namespace ibfs {
 
 // ---------------------------------------------------------------------------
-// Kernels
+// Kernels (the persistent kernel: persistent.cuh, one translation unit per
+// status width, persistent_w*.cu)
 // ---------------------------------------------------------------------------
-// THREADS x MINB fixes the register budget (65536 / (THREADS * MINB)) and
-// hence how many warps per SM hide the latency of the random gathers.
-template <int WORDS, int THREADS, int MINB>
-__global__ void __launch_bounds__(THREADS, MINB) persistent_kernel(Params p) {
-  __shared__ int s_dir, s_stop, s_err, s_maxl, s_dense;
-  __shared__ int32_t s_rows[kMaxWords * 32];
-  const int g = blockIdx.x / p.cpg;
-  const Team t = make_team(blockIdx.x % p.cpg, p.cpg);
-  const GroupBufs gb = p.groups[g];
-  Ctl* ctl = gb.ctl;
-  const unsigned nb = (unsigned)p.cpg;
-  const bool lead = (t.block == 0 && threadIdx.x == 0);
-  bool withhold = p.withhold && t.block == 0 && g == 0;
-  const long long vpad = (p.V + 31) & ~31LL;
-
-#define BARRIER()                                                   \
-  do {                                                              \
-    if (!team_barrier(ctl, nb, p.timeout_ns, withhold)) return;     \
-    withhold = false;                                               \
-  } while (0)
-
-  for (int b = g; b < p.nbatches; b += p.G) {
-    const long long k0 = (long long)b * p.C;
-    const int n_b = (int)min((long long)p.C, p.n_total - k0);
-    zero_words(gb.last, vpad * WORDS, t);
-    zero_words(gb.curr, vpad * WORDS, t);
-    zero_words(gb.chg, 2 * p.chg_stride, t);
-    load_rows(p, b, n_b, s_rows);
-    if (lead) {
-      memset(&ctl->par[0], 0, sizeof(Par) * 2);
-      memset(&ctl->qc[0][0], 0, sizeof(ctl->qc));
-    }
-    BARRIER();
-    seed_phase<WORDS>(p, gb, p.src + k0, n_b, t);
-    BARRIER();
-    inspect_phase<WORDS, true>(p, gb, &ctl->par[0], n_b, 0, true, false, t);
-    BARRIER();
-    int level = 0, cur_dir = kDirTD, max_level = 0, td = 0, bu = 0;
-    unsigned long long m_u = (unsigned long long)p.E, teps = 0, prev_changed = 0;
-    unsigned long long t_lvl = global_ns(), t_mid = t_lvl;
-    int err = 0;
-    while (true) {
-      if (threadIdx.x == 0) {
-        const volatile Par* pr = &ctl->par[level & 1];
-        const unsigned long long changed = pr->changed, mf = pr->mf, cdeg = pr->cdeg;
-        teps += pr->teps;
-        m_u = m_u > cdeg ? m_u - cdeg : 0ull;
-        int stop = 0;
-        if (pr->range_err) { stop = 1; err = 3; }
-        else if (changed == 0) stop = 1;
-        else if (level + 1 > p.max_levels) { stop = 1; err = 3; }
-        if (changed && !pr->range_err) max_level = level;
-        const int nd = choose_dir(level + 1, cur_dir, p.switch_level, p.alpha, p.beta,
-                                  changed, prev_changed, mf, m_u, p.V);
-        prev_changed = changed;
-        if (t.block == 0) {
-          if (level < p.lrec_cap) {
-            LevelRec r;
-            r.batch = b; r.level = level; r.dir = level == 0 ? -1 : cur_dir; r.pad = 0;
-            r.frontier = (long long)changed; r.frontier_edges = (long long)mf;
-            const unsigned long long t_now = global_ns();
-            r.expand_ns = (long long)(t_mid - t_lvl);
-            r.inspect_ns = (long long)(t_now - t_mid);
-            t_lvl = t_now;
-            p.lrec[(size_t)b * p.lrec_cap + level] = r;
-          }
-          if (!stop) {
-            memset((void*)&ctl->par[(level + 1) & 1], 0, sizeof(Par));
-            ctl->qc[level & 1][0] = ctl->qc[level & 1][1] = ctl->qc[level & 1][2] = 0;
-          }
-        }
-        s_dir = nd;
-        s_stop = stop;
-        s_err = err;
-        s_maxl = max_level;
-        s_dense = inspect_dense(mf, p.V) ? 1 : 0;
-      }
-      __syncthreads();
-      const int stop = s_stop;
-      cur_dir = s_dir;
-      err = s_err;
-      const bool dense = s_dense != 0;
-      __syncthreads();
-      if (stop) break;
-      level++;
-      bool continue_inspect = false;
-      zero_plane_if_first(p, gb, level, t);
-      if (cur_dir == kDirTD) {
-        td++;
-        qbuild_phase(p, gb, level, ctl->qc[level & 1], t);
-        BARRIER();
-        td_phase<WORDS>(p, gb, level, ctl->qc[level & 1], t);
-      } else {
-        bu++;
-        bu_phase<WORDS>(p, gb, level, ctl->par[(level - 1) & 1].fmask,
-                        &ctl->par[level & 1].hq_cnt, t);
-        BARRIER();
-        if (__ldcg(&ctl->par[level & 1].hq_cnt) > 0) {  // same value in every CTA
-          bu_defer_phase<WORDS>(p, gb, level, ctl->par[(level - 1) & 1].fmask,
-                                &ctl->par[level & 1].hq_cnt, t);
-          BARRIER();
-        }
-        if (lead) t_mid = global_ns();
-        continue_inspect = true;
-      }
-      if (!continue_inspect) {
-        BARRIER();
-        if (lead) t_mid = global_ns();
-      }
-      inspect_phase<WORDS, true>(p, gb, &ctl->par[level & 1], n_b, level,
-                                 level <= depth_limit(p.db), dense, t);
-      BARRIER();
-    }
-    if (err) {
-      if (lead) {
-        atomicCAS(&ctl->err, 0, err);
-        p.brec[b].err = err;
-      }
-      return;
-    }
-    output_phase<WORDS>(p, gb, batch_depth(p, b), s_rows, n_b, s_maxl, t);
-    if (lead && level + 1 < p.lrec_cap) {
-      // one extra record per batch: dir 2 = the output pass
-      LevelRec r;
-      r.batch = b; r.level = level + 1; r.dir = 2; r.pad = 0;
-      r.frontier = 0; r.frontier_edges = 0;
-      r.expand_ns = (long long)(global_ns() - t_lvl);
-      r.inspect_ns = 0;
-      p.lrec[(size_t)b * p.lrec_cap + level + 1] = r;
-    }
-    if (lead) {
-      BatchRec r;
-      r.levels = level;
-      r.max_level = max_level;
-      r.td = td;
-      r.bu = bu;
-      r.teps = teps;
-      r.err = 0;
-      r.pad = 0;
-      p.brec[b] = r;
-    }
-    BARRIER();
-  }
-#undef BARRIER
-}
-
 // ---- plain schedule: one kernel per phase, the whole grid is the team ----
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_seed(Params p, int b) {
@@ -405,22 +260,12 @@ static size_t group_bytes(int64_t V, int64_t E, int words, int C, int db, int lr
 // arguments below).
 static const int kOccThreads[4] = {512, 256, 256, 512};
 
-template <int WORDS>
-static const void* persistent_fn(int level) {
-  switch (level) {
-    case 1: return (const void*)persistent_kernel<WORDS, 256, 6>;
-    case 2: return (const void*)persistent_kernel<WORDS, 256, 8>;
-    case 3: return (const void*)persistent_kernel<WORDS, 512, 1>;
-    default: return (const void*)persistent_kernel<WORDS, 512, 2>;
-  }
-}
-
 static const void* persistent_for(int words, int level = 0) {
   switch (words) {
-    case 1: return persistent_fn<1>(level);
-    case 2: return persistent_fn<2>(level);
-    case 4: return persistent_fn<4>(level);
-    default: return persistent_fn<8>(level);
+    case 1: return persistent_fn_w32(level);
+    case 2: return persistent_fn_w64(level);
+    case 4: return persistent_fn_w128(level);
+    default: return persistent_fn_w256(level);
   }
 }
 
@@ -492,6 +337,73 @@ static ibfs_status ensure_workspace(ibfs_graph* g, const RunPlan& rp, const ibfs
   }
   return IBFS_OK;
 }
+
+}  // namespace ibfs
+
+namespace ibfs {
+// The launch parameters that depend only on the resident graph and the
+// options (the run's sources, rows, output, groups and records are left
+// null/zero for the caller).
+void fill_graph_params(const ibfs_graph* g, const ibfs_opts& o, int words, int threads,
+                       Params* pp) {
+  Params& p = *pp;
+  std::memset(&p, 0, sizeof(p));
+  p.beg = g->beg.as<int64_t>();
+  p.col = g->col.as<int32_t>();
+  p.V = g->V;
+  p.E = g->E;
+  p.nchg = (g->V + 31) / 32;
+  p.chg_stride = (p.nchg + 127) & ~127LL;  // whole 128-word blocks (vector bitmap walks)
+  p.plane_stride = (long long)((g->V + 31) & ~31LL) * words;
+  p.sml = o.sml_shed;
+  p.lrg = o.lrg_shed;
+  p.chunk = threads * 4;
+  p.but = o.bu_thread_max > 0 ? o.bu_thread_max : 32;
+  p.switch_level = o.switch_level;
+  p.alpha = o.alpha;
+  p.beta = o.beta;
+  p.max_levels = o.max_levels ? o.max_levels : 65534;
+  p.timeout_ns = (unsigned long long)(o.timeout_ms ? o.timeout_ms : 10000) * 1000000ull;
+  p.withhold = o.debug_withhold;
+  p.hub_t = kHubScan;
+  p.bu_filter = o.bu_filter > 0 ? 1 : 0;
+  p.col_vec = 1;
+  p.vmap = g->vmap.as<int32_t>();
+  // Degrees are non-increasing in the internal order: the vertices above the
+  // thread-path limit form a prefix (rounded up to whole warps).  When each
+  // warp owns only a few 32-vertex ranges of the bottom-up sweep (small
+  // graphs), the warps that own the hub ranges would be the critical path,
+  // so the prefix then gets one warp per vertex; on large graphs the ranges
+  // average out and the per-lane sweep is faster (R-MAT scale 16: 1.26 ->
+  // 0.45 ms per run with the prefix pass; scale 24: 34.8 vs 40.7 ms without
+  // and with it).
+  const int64_t ranges_per_warp = ((g->V + 31) / 32) / std::max<int64_t>(1, (int64_t)g->sms * 64);
+  if (ranges_per_warp < 8) {
+    int64_t lo = 0, hi = g->V;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) / 2;
+      if (g->dbeg_host[(size_t)mid + 1] - g->dbeg_host[(size_t)mid] > p.but) lo = mid + 1;
+      else hi = mid;
+    }
+    p.big_prefix = std::min<int64_t>((lo + 31) & ~31LL, (g->V + 31) & ~31LL);
+  }
+}
+
+// The output pointer and the store widths its alignment allows.
+void set_output_params(const ibfs_graph* g, int C, uint8_t* dout, Params* p) {
+  p->out = dout;
+  p->vec_out = (C % 4 == 0) && ((reinterpret_cast<uintptr_t>(dout) & 3) == 0);
+  p->vec_sm = (g->V % 16 == 0 && (reinterpret_cast<uintptr_t>(dout) & 15) == 0)  ? 16
+              : (g->V % 4 == 0 && (reinterpret_cast<uintptr_t>(dout) & 3) == 0) ? 4
+                                                                               : 0;
+}
+
+int graph_sms(const ibfs_graph* g) { return g->sms; }
+int64_t graph_defer_cap(const ibfs_graph* g) { return g->defer_cap; }
+const int32_t* graph_new_of_old(const ibfs_graph* g) { return g->new_of_old.data(); }
+}  // namespace ibfs
+
+namespace ibfs {
 
 // Key of a captured persistent run.  A captured graph holds raw addresses:
 // the kernel's Params (CSR, sources, rows, output, group table, records,
@@ -1092,14 +1004,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     hgb[i].planes = m.planes.as<uint32_t>();
   }
   Params p;
-  std::memset(&p, 0, sizeof(p));
-  p.beg = g->beg.as<int64_t>();
-  p.col = g->col.as<int32_t>();
-  p.V = g->V;
-  p.E = g->E;
-  p.nchg = (g->V + 31) / 32;
-  p.chg_stride = (p.nchg + 127) & ~127LL;  // whole 128-word blocks (vector bitmap walks)
-  p.plane_stride = (long long)((g->V + 31) & ~31LL) * rp.words;
+  fill_graph_params(g, o, rp.words, rp.threads, &p);
   p.src = g->d_src.as<int32_t>();
   p.out_row = g->d_outrow.as<int32_t>();
   p.n_total = n;
@@ -1109,47 +1014,11 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   p.cpg = rp.cpg;
   p.db = db;
   p.layout = layout;
-  p.out = dout;
-  p.sml = o.sml_shed;
-  p.lrg = o.lrg_shed;
-  p.chunk = rp.threads * 4;
-  p.but = o.bu_thread_max > 0 ? o.bu_thread_max : 32;
-  p.switch_level = o.switch_level;
-  p.alpha = o.alpha;
-  p.beta = o.beta;
-  p.max_levels = o.max_levels ? o.max_levels : 65534;
-  p.timeout_ns = (unsigned long long)(o.timeout_ms ? o.timeout_ms : 10000) * 1000000ull;
-  p.withhold = o.debug_withhold;
   p.groups = g->d_groups.as<GroupBufs>();
   p.brec = g->d_brec.as<BatchRec>();
   p.lrec = g->d_lrec.as<LevelRec>();
   p.lrec_cap = kLrecCap;
-  p.vec_out = (rp.C % 4 == 0) && ((reinterpret_cast<uintptr_t>(dout) & 3) == 0);
-  p.hub_t = kHubScan;
-  p.bu_filter = o.bu_filter > 0 ? 1 : 0;
-  p.col_vec = 1;
-  p.vmap = g->vmap.as<int32_t>();
-  // Degrees are non-increasing in the internal order: the vertices above the
-  // thread-path limit form a prefix (rounded up to whole warps).  When each
-  // warp owns only a few 32-vertex ranges of the bottom-up sweep (small
-  // graphs), the warps that own the hub ranges would be the critical path,
-  // so the prefix then gets one warp per vertex; on large graphs the ranges
-  // average out and the per-lane sweep is faster (R-MAT scale 16: 1.26 ->
-  // 0.45 ms per run with the prefix pass; scale 24: 34.8 vs 40.7 ms without
-  // and with it).
-  const int64_t ranges_per_warp = ((g->V + 31) / 32) / std::max<int64_t>(1, (int64_t)g->sms * 64);
-  if (ranges_per_warp < 8) {
-    int64_t lo = 0, hi = g->V;
-    while (lo < hi) {
-      const int64_t mid = (lo + hi) / 2;
-      if (g->dbeg_host[(size_t)mid + 1] - g->dbeg_host[(size_t)mid] > p.but) lo = mid + 1;
-      else hi = mid;
-    }
-    p.big_prefix = std::min<int64_t>((lo + 31) & ~31LL, (g->V + 31) & ~31LL);
-  }
-  p.vec_sm = (g->V % 16 == 0 && (reinterpret_cast<uintptr_t>(dout) & 15) == 0)  ? 16
-             : (g->V % 4 == 0 && (reinterpret_cast<uintptr_t>(dout) & 3) == 0) ? 4
-                                                                              : 0;
+  set_output_params(g, rp.C, dout, &p);
   // Per-batch done flags of the device loop, in mapped host memory, grown in
   // powers of two so that their address (baked into cached graphs) stays put.
   if ((size_t)rp.nbatches > g->done_cap) {

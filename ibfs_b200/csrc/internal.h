@@ -1,6 +1,7 @@
 // internal.h -- declarations shared by the host C++ and CUDA sources of libibfs.
 #pragma once
 #include <cstdint>
+#include <algorithm>
 #include <cstddef>
 #include <string>
 #include <vector>
@@ -47,6 +48,12 @@ void groupby_host_maxhub(const int64_t* beg, const int32_t* col, int64_t V,
 
 namespace ibfs {
 struct Params;
+// persistent_w*.cu: the persistent kernel's address for a status width and an
+// occupancy level (0: 512 x 2, 1: 256 x 6, 2: 256 x 8, 3: 512 x 1).
+const void* persistent_fn_w32(int level);
+const void* persistent_fn_w64(int level);
+const void* persistent_fn_w128(int level);
+const void* persistent_fn_w256(int level);
 // engine.cu: launch helpers shared with the static-scratch entry point.
 cudaError_t launch_persistent_params(const Params& p, int words, int grid, int threads,
                                      size_t smem, cudaStream_t s);
@@ -68,6 +75,81 @@ ibfs_status run_rows(ibfs_graph* g, const int32_t* src, const int32_t* rows, int
 int graph_device(const ibfs_graph* g);
 const int64_t* graph_host_beg(const ibfs_graph* g);
 const int32_t* graph_host_col(const ibfs_graph* g);
+int graph_sms(const ibfs_graph* g);
+int64_t graph_defer_cap(const ibfs_graph* g);
+const int32_t* graph_new_of_old(const ibfs_graph* g);  // caller id -> internal id (host)
+// Launch parameters that depend only on the graph and the options, and the
+// output pointer with the store widths its alignment allows.
+void fill_graph_params(const ibfs_graph* g, const ibfs_opts& o, int words, int threads,
+                       Params* p);
+void set_output_params(const ibfs_graph* g, int C, uint8_t* dout, Params* p);
+}  // namespace ibfs
+
+namespace ibfs {
+// serve_loop.cu: the serving schedule -- the device-loop graph of G groups
+// fed from a work queue in mapped host memory (Params::q_*).  The host
+// publishes batches of already grouped sources whose depths go to rows of a
+// device arena while the graph runs; each group claims the next published
+// batch when it finishes one.  Not thread safe: one host thread drives it.
+class ServeLoop {
+ public:
+  struct Done {
+    int slot;
+    int32_t err;         // 0, or the batch's ibfs_status
+    uint64_t teps;       // traversed edges of the batch
+    int32_t max_level;
+  };
+  ~ServeLoop();
+  // G groups, `slots` queue slots of C sources each, depths (db bytes) to
+  // source-major rows of `arena` (V * db bytes per row).
+  ibfs_status init(ibfs_graph* g, const ibfs_opts& o, int G, int slots, void* arena, int db);
+  int capacity() const { return C_; }
+  int groups() const { return G_; }
+  // whether the next slot in publishing order is free
+  bool can_publish() const {
+    return std::find(free_.begin(), free_.end(), (int)(published_ % slots_)) != free_.end();
+  }
+  // published batches that no group has claimed yet
+  int unclaimed() const;
+  // slots published and not yet reported done
+  int in_flight() const { return (int)busy_.size(); }
+  // Publish one batch (caller ids, 1..C sources, their arena rows); returns
+  // the slot, or -1 when no slot is free.
+  int publish(const int32_t* src, const int32_t* rows, int n);
+  // Launch the graph when it is not running and a published batch waits.
+  // Returns true when a launch was issued.
+  ibfs_status pump(bool* launched);
+  // Batches finished since the last call.
+  void harvest(std::vector<Done>* out);
+  // Whether the graph is running.
+  bool running();
+  // Wait for the running graph to end (every group finds the queue empty).
+  ibfs_status drain();
+  double busy_ms() const { return busy_ms_; }
+  int64_t launches() const { return launches_; }
+  void release();
+
+ private:
+  ibfs_graph* g_ = nullptr;
+  int device_ = 0, C_ = 0, slots_ = 0, G_ = 0, words_ = 0, db_ = 1;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
+  bool live_ = false;
+  double busy_ms_ = 0.0;
+  int64_t launches_ = 0;
+  long long published_ = 0;
+  // mapped host memory: tail, n, src, rows, state, records
+  void* host_ = nullptr;
+  long long* h_tail_ = nullptr;
+  int32_t *h_n_ = nullptr, *h_src_ = nullptr, *h_rows_ = nullptr, *h_state_ = nullptr;
+  void* h_brec_ = nullptr;
+  // device memory: workspace of the G groups, slot copies, claim counter
+  std::vector<void*> dev_;
+  std::vector<int> free_;   // free slots
+  std::vector<int> busy_;   // published, not yet harvested
+  void* dalloc(size_t bytes);
+};
 }  // namespace ibfs
 
 namespace ibfs {

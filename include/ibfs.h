@@ -230,9 +230,12 @@ typedef struct ibfs_server_opts {
     int64_t arena_bytes;     /* device memory for per-query depth rows
                                 (0: a quarter of the free device memory)       */
     int32_t max_waiting;     /* queued submissions beyond this: IBFS_ERR_BUSY  */
-    int32_t round_batches;   /* batches of `concurrent` sources per round      */
-    int32_t max_wait_us;     /* a partial round waits this long for sources    */
-    int32_t groupby;         /* regroup each round's sources with GroupBy      */
+    int32_t round_batches;   /* batches traversed at once (the device loop's
+                                concurrent groups); also the most batches'
+                                worth of sources regrouped together            */
+    int32_t max_wait_us;     /* a partial batch waits this long for sources
+                                (only while no published batch is unclaimed)   */
+    int32_t groupby;         /* regroup pending sources with GroupBy           */
     int32_t reserved[6];
 } ibfs_server_opts;
 typedef struct ibfs_query_info {
@@ -241,12 +244,19 @@ typedef struct ibfs_query_info {
     double queue_ms;         /* submission to the first round that included it  */
     int32_t status;          /* ibfs_status of the query                        */
     int32_t depth_bytes;
+    double delivered_ms;     /* submission to depths in the caller's buffer
+                                (the poll or wait that collected the query)     */
 } ibfs_query_info;
 typedef struct ibfs_server_stats {
-    int64_t submitted, completed, refused, rounds, sources, traversed_edges;
-    double busy_ms;          /* device time of all rounds                       */
+    int64_t submitted, completed, refused;
+    int64_t rounds;          /* batches traversed                               */
+    int64_t sources, traversed_edges;
+    double busy_ms;          /* device time of the serving graph's launches     */
     double wall_ms;          /* since creation                                  */
     int64_t arena_rows, arena_rows_used;
+    int64_t launches;        /* serving-graph launches: batches published while
+                                the graph runs join it, so launches < rounds
+                                under load                                      */
 } ibfs_server_stats;
 void ibfs_server_opts_default(ibfs_server_opts *o);
 /* Start a server (worker thread) on a resident graph. */

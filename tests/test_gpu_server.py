@@ -82,3 +82,64 @@ def test_refusals(graph):
         with pytest.raises(ib.IbfsError) as ei:
             srv.poll(123456789, 1)
         assert ei.value.status == 10
+
+
+def test_batches_join_running_graph(graph):
+    """Batches published while the serving graph runs are claimed by its
+    groups without a new launch, and every result still equals the oracle."""
+    beg, col, g = graph
+    qs = [ib.sample_sources(beg, col, 128, seed=300 + i) for i in range(16)]
+    with ib.Server(g, width=128, round_batches=2, max_wait_us=0) as srv:
+        st0 = srv.stats()
+        ids = [srv.submit(q) for q in qs]
+        res = [srv.wait(qid, len(q))[0] for q, qid in zip(qs, ids)]
+        st = srv.stats()
+    assert st["rounds"] - st0["rounds"] == 16
+    assert st["launches"] - st0["launches"] < 16 - 2, st
+    for q, d in zip(qs, res):
+        ref, _ = oracle.bfs(beg, col, q)
+        assert np.array_equal(d, ref)
+
+
+def test_late_queries_overlap_early_ones(graph):
+    """A query submitted while an earlier one is still on the GPU starts
+    before that one completes (its queue time is shorter than the earlier
+    query's remaining latency) and both match the oracle."""
+    beg, col, g = graph
+    early = ib.sample_sources(beg, col, 256, seed=401)
+    late = ib.sample_sources(beg, col, 8, seed=402)
+    with ib.Server(g, width=32, round_batches=4, max_wait_us=0) as srv:
+        qe = srv.submit(early)   # 8 batches of 32 over 4 groups
+        ql = srv.submit(late)
+        de, ie = srv.wait(qe, len(early))
+        dl, il = srv.wait(ql, len(late))
+    ref_e, _ = oracle.bfs(beg, col, early)
+    ref_l, _ = oracle.bfs(beg, col, late)
+    assert np.array_equal(de, ref_e) and np.array_equal(dl, ref_l)
+    assert il["queue_ms"] <= ie["latency_ms"]
+    assert il["delivered_ms"] >= il["latency_ms"]
+
+
+def test_batch_error_stays_with_its_query():
+    """One-byte depths past level 254 fail the query whose batch hit them;
+    the server keeps serving and the next query is exact."""
+    V_path, k = 400, 8
+    edges = [(i, i + 1) for i in range(V_path - 1)]
+    edges += [(V_path + a, V_path + b) for a in range(k) for b in range(a + 1, k)]
+    beg, col = ib.csr_from_edges(np.array([e[0] for e in edges], np.int32),
+                                 np.array([e[1] for e in edges], np.int32), V_path + k)
+    g = ib.Graph.from_csr(beg, col)
+    try:
+        with ib.Server(g, width=32, depth_bytes=1, round_batches=1, max_wait_us=0) as srv:
+            qa = srv.submit(np.array([0], np.int32))
+            with pytest.raises(ib.IbfsError) as ei:
+                srv.wait(qa, 1)
+            assert ei.value.status == 3
+            src = np.array([V_path, V_path + 3], np.int32)
+            qb = srv.submit(src)
+            depth, info = srv.wait(qb, 2)
+            assert info["status"] == 0
+            ref, _ = oracle.bfs(beg, col, src)
+            assert np.array_equal(depth, ref)
+    finally:
+        g.close()
