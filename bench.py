@@ -365,15 +365,16 @@ def run_ours(args, cfg):
         res = step()
     stream.synchronize()
     # The autotuner (coordinate descent over width, alpha/beta, queue
-    # thresholds and groups, each trial a real run) on a sample of the
-    # sources; the timed run then uses the options it picked, and the same
-    # run with the library defaults is timed beside it.  Every rank tunes on
+    # thresholds and groups, each trial a real run) on the run's sources
+    # (or a sample of them); the timed run then uses the options it picked,
+    # and the same run with the library defaults is timed beside it.  Every rank tunes on
     # its own sample (deterministic per rank, no collective).
     tuned = None
     if args.tune:
         t_tune = time.perf_counter()
         base_opts = ib.Opts.from_buffer_copy(opts)
-        best, _, trials = g.autotune(src[:min(n, args.tune_sample)], base_opts, reps=2)
+        k_tune = n if args.tune_sample <= 0 else min(n, args.tune_sample)
+        best, _, trials = g.autotune(src[:k_tune], base_opts, reps=2)
         t_tune = time.perf_counter() - t_tune
         ms_def = []
         for _ in range(3):
@@ -385,7 +386,7 @@ def run_ours(args, cfg):
         for _ in range(max(args.warmup, 3)):
             res = step()
         stream.synchronize()
-        tuned = {"sample_sources": int(min(n, args.tune_sample)), "trials": len(trials),
+        tuned = {"sample_sources": int(k_tune), "trials": len(trials),
                  "tune_s": round(t_tune, 2),
                  "chosen": {"width": opts.width, "alpha": opts.alpha, "beta": opts.beta,
                             "sml_shed": opts.sml_shed, "lrg_shed": opts.lrg_shed,
@@ -503,7 +504,10 @@ def run_ours(args, cfg):
         ee_all = sum_over_ranks(float(ee), world)
         e2e = {"value": round(ee_all / t_e / 1e9, 4), "unit": "GTEPS",
                "h2d_bytes_per_step": int(n * 4), "d2h_bytes_per_step": int(n * V),
-               "steps": e_steps}
+               "steps": e_steps,
+               # the depth rows cross PCIe once: the e2e bound is this copy rate
+               "d2h_gbs": round(n * V * e_steps / t_e / 1e9, 2),
+               "ms_per_step": round(t_e / e_steps * 1e3, 3)}
         ok = np.array_equal(host.numpy()[0], out[0].cpu().numpy())
         e2e["matches_device_run"] = bool(ok)
         del host
@@ -662,7 +666,8 @@ def main():
                     help="autotune on a sample before timing (default: on for c3, which "
                          "is quoted autotuned)")
     ap.add_argument("--no-tune", dest="tune", action="store_false")
-    ap.add_argument("--tune-sample", type=int, default=256)
+    ap.add_argument("--tune-sample", type=int, default=0,
+                    help="sources the autotuner times (0: all of the run's sources)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-roofline", action="store_true")

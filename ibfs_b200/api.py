@@ -43,7 +43,8 @@ class Opts(C.Structure):
         ("depth_bytes", C.c_int32), ("groups", C.c_int32), ("threads", C.c_int32),
         ("ctas_per_sm", C.c_int32), ("use_graph", C.c_int32), ("timeout_ms", C.c_int32),
         ("max_levels", C.c_int32), ("debug_withhold", C.c_int32), ("occupancy", C.c_int32),
-        ("bu_filter", C.c_int32), ("bu_thread_max", C.c_int32), ("reserved", C.c_int32 * 4),
+        ("bu_filter", C.c_int32), ("bu_thread_max", C.c_int32), ("td_stage", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 

@@ -85,8 +85,14 @@ extern "C" ibfs_status ibfs_autotune(ibfs_graph* g, const int32_t* src, int64_t 
     return s;
   }
   note(cur);
+  // A knob moves off its current value only for a gain above kMinGain: two
+  // timings of the same options differ by up to about 1 %, and chasing that
+  // noise can leave a choice that is slower on the full workload.
+  constexpr double kMinGain = 0.01;
   auto try_set = [&](auto mutate, int count) -> ibfs_status {
     Trial bestt = cur;
+    bestt.gteps = cur.gteps * (1.0 + kMinGain);
+    bool moved = false;
     for (int i = 0; i < count; i++) {
       ibfs_opts o = cur.o;
       if (!mutate(o, i)) continue;
@@ -96,9 +102,12 @@ extern "C" ibfs_status ibfs_autotune(ibfs_graph* g, const int32_t* src, int64_t 
         continue;  // a combination that does not fit: skip it
       if (st != IBFS_OK) return st;
       note(t);
-      if (t.gteps > bestt.gteps) bestt = t;
+      if (t.gteps > bestt.gteps) {
+        bestt = t;
+        moved = true;
+      }
     }
-    cur = bestt;
+    if (moved) cur = bestt;
     return IBFS_OK;
   };
   const int widths[] = {32, 64, 128, 256};

@@ -134,7 +134,10 @@ struct Params {
   int vec_out;  // vertex-major rows allow 4-byte stores (n_b*db % 4 == 0, aligned base)
   int vec_sm;   // source-major rows allow vector stores of this many bytes: 16 (V % 16
                 // == 0, 16-byte aligned base), 4 (V % 4 == 0, 4-byte aligned) or 0
-  int bu_filter;    // bottom-up skips neighbours outside the previous frontier
+  int td_stage;     // top-down stages large vertices' chunks by bulk copies
+  int bu_filter;    // bottom-up skips neighbours outside the previous frontier:
+                    // 1 always, 0 never, -1 on levels whose previous frontier
+                    // is small (bu_filter_level)
   int col_vec;      // col is 16-byte aligned and padded by 4 entries (vector reads)
   int hub_t;        // bottom-up: a warp scans at most hub_t neighbours of a vertex;
                     // a hub still missing bits defers the rest in chunks
@@ -172,6 +175,35 @@ struct Params {
 #define IBFS_BU_STEP 4
 #endif
 constexpr int kBuStep = IBFS_BU_STEP;
+// Steps of kBuStep neighbours a big vertex (degree above the thread-path
+// limit) scans on its own lane before the warp takes it (0: none).
+#ifndef IBFS_BU_PEEK
+#define IBFS_BU_PEEK 2
+#endif
+constexpr int kBuPeek = IBFS_BU_PEEK;
+// Bottom-up frontier filter.  A neighbour u that did not change at level L-1
+// cannot give v a bit it lacks at level L: every bit u held before L-1
+// reached v by L-1 already (BFS distances of adjacent vertices differ by at
+// most one).  So the scan may skip, exactly, every neighbour outside the
+// level-(L-1) changed bitmap.  The bitmap test costs a lookup per neighbour;
+// it can pay off when the previous frontier is a small part of the graph
+// (the tail levels of a traversal), not when it is a large part.
+constexpr long long kFilterDiv = 16;  // auto: filter when prev frontier < V / 16
+__host__ __device__ inline bool bu_filter_level(int mode, unsigned long long prev_changed,
+                                                long long V) {
+  if (mode >= 0) return mode > 0;
+  return (long long)prev_changed * kFilterDiv < V;
+}
+
+// Whether u is in the previous level's changed bitmap; through L1 when the
+// pass runs as a kernel of its own (RO: nothing writes that bitmap while it
+// runs), else through L2 (the persistent kernel rewrites it at later levels).
+template <bool RO>
+__device__ __forceinline__ bool in_front(const uint32_t* front, int32_t u) {
+  const uint32_t w = RO ? __ldg(front + (u >> 5)) : __ldcg(front + (u >> 5));
+  return (w >> (u & 31)) & 1u;
+}
+
 constexpr int kHubScan = 1024;   // neighbours one warp scans before deferring
 constexpr int kHubChunk = 2048;  // edges per deferred chunk (one CTA each)
 
@@ -661,76 +693,249 @@ __device__ inline void qbuild_phase(const Params& p, const GroupBufs& gb, int le
   }
 }
 
-// One top-down edge: push the frontier word P of v into neighbour u.
-// The status read goes to L2 (ld.cg): it only filters atomics, a stale
-// value has fewer bits and just costs one more atomic.
+// Fire-and-forget ORs (red: no value comes back, so nothing waits on them).
+__device__ __forceinline__ void red_or_u32(uint32_t* p, uint32_t x) {
+  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(x) : "memory");
+}
+__device__ __forceinline__ void red_or_u64(unsigned long long* p, unsigned long long x) {
+  asm volatile("red.relaxed.gpu.global.or.b64 [%0], %1;" ::"l"(p), "l"(x) : "memory");
+}
+
+// Top-down edges: push the frontier word P of v into neighbours u[0..cnt).
+// The status reads of all cnt neighbours are issued before any of them is
+// used, so one thread has cnt gathers in flight instead of one.
+// The status read s (through L2) decides everything: every level starts
+// with curr == last, so bits of P missing from s are missing from last[u],
+// and once ORed in (by this thread or a concurrent one) u has changed at
+// this level.  So the ORs into curr[u] and into the changed bitmap are
+// reductions whose old value is never needed: the thread issues them and
+// goes on instead of waiting for L2 round trips.  A stale s (fewer bits)
+// costs at most one redundant OR.
+constexpr int kTdStep = 4;  // edges one thread has in flight
 template <int WORDS>
-__device__ __forceinline__ void td_push(const GroupBufs& gb, uint32_t* chg, int32_t u,
-                                        const uint32_t (&P)[WORDS]) {
-  uint32_t s[WORDS];
-  ld_status<WORDS>(gb.curr + (size_t)u * WORDS, s);
-  bool need = false;
+__device__ __forceinline__ void td_push_n(const GroupBufs& gb, uint32_t* chg,
+                                          const int32_t (&u)[kTdStep], int cnt,
+                                          const uint32_t (&P)[WORDS]) {
+  uint32_t s[kTdStep][WORDS];
 #pragma unroll
-  for (int k = 0; k < WORDS; k++) need |= (P[k] & ~s[k]) != 0u;
-  if (!need) return;
-  bool changed = false;
-  if constexpr (WORDS == 1) {
-    const uint32_t old = atomicOr(gb.curr + u, P[0]);
-    changed = (old & P[0]) != P[0];
-  } else {
-    unsigned long long* q = reinterpret_cast<unsigned long long*>(gb.curr + (size_t)u * WORDS);
+  for (int i = 0; i < kTdStep; i++) {
+    if (i < cnt) {
+      ld_status<WORDS>(gb.curr + (size_t)u[i] * WORDS, s[i]);
+    } else {
 #pragma unroll
-    for (int k = 0; k < WORDS / 2; k++) {
-      const uint32_t n0 = P[2 * k] & ~s[2 * k], n1 = P[2 * k + 1] & ~s[2 * k + 1];
-      if (n0 | n1) {
-        const unsigned long long pw = ((unsigned long long)P[2 * k + 1] << 32) | P[2 * k];
-        const unsigned long long old = atomicOr(q + k, pw);
-        changed |= (old & pw) != pw;
-      }
+      for (int k = 0; k < WORDS; k++) s[i][k] = 0xFFFFFFFFu;
     }
   }
-  if (changed) {
-    uint32_t* cw = chg + (u >> 5);
-    const uint32_t bit = 1u << (u & 31);
-    if (!(__ldcg(cw) & bit)) atomicOr(cw, bit);
+#pragma unroll
+  for (int i = 0; i < kTdStep; i++) {
+    bool need = false;
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) need |= (P[k] & ~s[i][k]) != 0u;
+    if (!need) continue;
+    if constexpr (WORDS == 1) {
+      red_or_u32(gb.curr + u[i], P[0]);
+    } else {
+      unsigned long long* q = reinterpret_cast<unsigned long long*>(gb.curr + (size_t)u[i] * WORDS);
+#pragma unroll
+      for (int k = 0; k < WORDS / 2; k++) {
+        const uint32_t n0 = P[2 * k] & ~s[i][2 * k], n1 = P[2 * k + 1] & ~s[i][2 * k + 1];
+        if (n0 | n1) red_or_u64(q + k, ((unsigned long long)P[2 * k + 1] << 32) | P[2 * k]);
+      }
+    }
+    red_or_u32(chg + (u[i] >> 5), 1u << (u[i] & 31));
   }
+}
+
+// ---- bulk-copy (TMA) staging of large vertices' adjacency chunks ---------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// One untiled bulk copy global -> shared (both addresses 16-byte aligned,
+// bytes a multiple of 16), completing on `bar`.  The source is this GPU's
+// own CSR; no multicast.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for phase `parity` of `bar` (each try_wait suspends the
+// thread for a while in hardware; kMbarTries of them is seconds).
+constexpr long long kMbarTries = 1LL << 22;
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  for (long long i = 0; i < kMbarTries; i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+constexpr int kStageInts = 2048 + 8;  // one chunk (threads*4 <= 2048) plus alignment slack
+
+// The column-id range [a0, a1) that covers chunk c of a large vertex with
+// 16-byte aligned ends (col is 16-byte aligned and padded by 4 entries).
+__device__ __forceinline__ void td_chunk(const Params& p, const GroupBufs& gb, int c, int32_t* v,
+                                         long long* b0, long long* b1, long long* a0,
+                                         long long* a1) {
+  const int2 d = gb.ql[c];
+  *v = d.x;
+  const long long e_end = p.beg[d.x + 1];
+  *b0 = p.beg[d.x] + (long long)d.y * p.chunk;
+  *b1 = min(e_end, *b0 + (long long)p.chunk);
+  *a0 = *b0 & ~3LL;
+  *a1 = (*b1 + 3) & ~3LL;
 }
 
 // ---------------------------------------------------------------------------
 // Phase: top-down expansion of level L over the three queues: one CTA per
 // chunk of a large vertex (td_expand_cta, expander.cuh:276-331), one warp
 // per medium vertex (td_expand_warp, expander.cuh:208-267), one thread per
-// small vertex (td_expand_thd, expander.cuh:140-199).
+// small vertex (td_expand_thd, expander.cuh:140-199).  Every thread takes
+// kTdStep edges at a time: their column ids first, then their statuses.
+// STAGE (the phase's own kernel, chunk <= 2048) with Params::td_stage: the
+// large vertices' chunks -- the hubs' adjacency -- are staged through shared
+// memory by bulk copies (TMA, cp.async.bulk), double-buffered: while the CTA
+// pushes one chunk's edges, the next chunk's column ids are already on
+// their way, so the pushes never wait for a column read.  Off by default:
+// on R-MAT scale 24 the top-down levels are bound by the random status
+// gathers, not by the column reads, and staging measured ~1 % slower.
 // ---------------------------------------------------------------------------
-template <int WORDS>
+template <int WORDS, bool STAGE = false>
 __device__ void td_phase(const Params& p, const GroupBufs& gb, int level, const int32_t* qc,
                          const Team& t) {
   uint32_t* chg = chg_at(gb, p, level);
   const int nS = __ldcg(qc + 0), nM = __ldcg(qc + 1), nL = __ldcg(qc + 2);
-  for (int c = t.block; c < nL; c += t.nblocks) {
-    const int2 d = gb.ql[c];
-    const int32_t v = d.x;
-    const long long e_end = p.beg[v + 1];
-    const long long b0 = p.beg[v] + (long long)d.y * p.chunk;
-    const long long b1 = min(e_end, b0 + (long long)p.chunk);
-    uint32_t P[WORDS];
-    ld_status<WORDS>(gb.last + (size_t)v * WORDS, P);
-    for (long long e = b0 + threadIdx.x; e < b1; e += blockDim.x)
-      td_push<WORDS>(gb, chg, p.col[e], P);
+  if (STAGE && p.td_stage) {
+    __shared__ __align__(128) int32_t s_col[2][kStageInts];
+    __shared__ __align__(8) unsigned long long s_bar[2];
+    __shared__ int s_fail;
+    if (threadIdx.x == 0) {
+      mbar_init(&s_bar[0], 1);
+      mbar_init(&s_bar[1], 1);
+      mbar_init_fence();
+      s_fail = 0;
+    }
+    __syncthreads();
+    auto issue = [&](int i) {  // thread 0: chunk i of this CTA into buffer i & 1
+      int32_t v;
+      long long b0, b1, a0, a1;
+      td_chunk(p, gb, t.block + i * t.nblocks, &v, &b0, &b1, &a0, &a1);
+      const unsigned bytes = (unsigned)((a1 - a0) * 4);
+      mbar_expect_tx(&s_bar[i & 1], bytes);
+      bulk_g2s(s_col[i & 1], p.col + a0, bytes, &s_bar[i & 1]);
+    };
+    int issued = 0;  // chunks whose copy thread 0 has started
+    if (threadIdx.x == 0 && t.block < nL) {
+      issue(0);
+      issued = 1;
+    }
+    for (int i = 0;; i++) {
+      const int c = t.block + i * t.nblocks;
+      if (c >= nL) break;
+      if (threadIdx.x == 0 && c + t.nblocks < nL) {
+        issue(i + 1);
+        issued = i + 2;
+      }
+      int32_t v;
+      long long b0, b1, a0, a1;
+      td_chunk(p, gb, c, &v, &b0, &b1, &a0, &a1);
+      uint32_t P[WORDS];
+      ld_status<WORDS>(gb.last + (size_t)v * WORDS, P);
+      if (!mbar_wait(&s_bar[i & 1], (unsigned)((i >> 1) & 1))) s_fail = 1;
+      __syncthreads();
+      if (s_fail) break;  // uniform
+      const int32_t* sc = s_col[i & 1] + (b0 - a0);
+      const int n = (int)(b1 - b0);
+      for (int j = threadIdx.x; j < n; j += kTdStep * blockDim.x) {
+        int32_t u[kTdStep];
+        int cnt = 0;
+#pragma unroll
+        for (int q = 0; q < kTdStep; q++) {
+          const int jq = j + q * (int)blockDim.x;
+          u[q] = jq < n ? sc[jq] : 0;
+          cnt += jq < n ? 1 : 0;
+        }
+        td_push_n<WORDS>(gb, chg, u, cnt, P);
+      }
+      __syncthreads();  // buffer i & 1 is read: the copy of chunk i + 2 may reuse it
+    }
+    if (s_fail && threadIdx.x == 0) {
+      // a copy did not complete in time: report it, and before the CTA's
+      // shared memory goes away, wait (bounded) for every copy it started
+      atomicCAS(&gb.ctl->err, 0, 6);
+      for (int i = 0; i < issued; i++) (void)mbar_wait(&s_bar[i & 1], (unsigned)((i >> 1) & 1));
+    }
+  } else {
+    for (int c = t.block; c < nL; c += t.nblocks) {
+      int32_t v;
+      long long b0, b1, a0, a1;
+      td_chunk(p, gb, c, &v, &b0, &b1, &a0, &a1);
+      uint32_t P[WORDS];
+      ld_status<WORDS>(gb.last + (size_t)v * WORDS, P);
+      for (long long e = b0 + threadIdx.x; e < b1; e += (long long)kTdStep * blockDim.x) {
+        int32_t u[kTdStep];
+        int cnt = 0;
+#pragma unroll
+        for (int i = 0; i < kTdStep; i++) {
+          const long long ei = e + (long long)i * blockDim.x;
+          u[i] = ei < b1 ? __ldg(p.col + ei) : 0;
+          cnt += ei < b1 ? 1 : 0;
+        }
+        td_push_n<WORDS>(gb, chg, u, cnt, P);
+      }
+    }
   }
   for (long long i = t.warp; i < nM; i += t.nwarps) {
     const int32_t v = gb.qm[i];
     uint32_t P[WORDS];
     ld_status<WORDS>(gb.last + (size_t)v * WORDS, P);
     const long long b1 = p.beg[v + 1];
-    for (long long e = p.beg[v] + t.lane; e < b1; e += 32) td_push<WORDS>(gb, chg, p.col[e], P);
+    for (long long e = p.beg[v] + t.lane; e < b1; e += 32 * kTdStep) {
+      int32_t u[kTdStep];
+      int cnt = 0;
+#pragma unroll
+      for (int j = 0; j < kTdStep; j++) {
+        const long long ej = e + 32LL * j;
+        u[j] = ej < b1 ? __ldg(p.col + ej) : 0;
+        cnt += ej < b1 ? 1 : 0;
+      }
+      td_push_n<WORDS>(gb, chg, u, cnt, P);
+    }
   }
   for (long long i = t.tid; i < nS; i += t.nthreads) {
     const int32_t v = gb.qs[i];
     uint32_t P[WORDS];
     ld_status<WORDS>(gb.last + (size_t)v * WORDS, P);
     const long long b1 = p.beg[v + 1];
-    for (long long e = p.beg[v]; e < b1; e++) td_push<WORDS>(gb, chg, p.col[e], P);
+    for (long long e = p.beg[v]; e < b1; e += kTdStep) {
+      int32_t u[kTdStep];
+      const int cnt = (int)min((long long)kTdStep, b1 - e);
+#pragma unroll
+      for (int j = 0; j < kTdStep; j++) u[j] = j < cnt ? __ldg(p.col + e + j) : 0;
+      td_push_n<WORDS>(gb, chg, u, cnt, P);
+    }
   }
 }
 
@@ -742,7 +947,8 @@ __device__ void td_phase(const Params& p, const GroupBufs& gb, int level, const 
 // instead of holding one warp -- and the whole level -- for its adjacency.
 template <int WORDS, bool RO = false>
 __device__ void bu_defer_phase(const Params& p, const GroupBufs& gb, int level,
-                               const uint32_t* fmask_g, const int32_t* hq_cnt, const Team& t) {
+                               const uint32_t* fmask_g, const int32_t* hq_cnt, const Team& t,
+                               bool filt = false) {
   __shared__ uint32_t s_acc[32][kMaxWords];
   __shared__ uint32_t s_cur[kMaxWords];
   __shared__ int s_skip;
@@ -780,7 +986,7 @@ __device__ void bu_defer_phase(const Params& p, const GroupBufs& gb, int level,
     for (int k = 0; k < WORDS; k++) acc[k] = 0;
     for (long long e = b0 + threadIdx.x; e < b1; e += blockDim.x) {
       const int32_t u = p.col[e];
-      if (p.bu_filter && !((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u)) continue;
+      if (filt && !in_front<RO>(front, u)) continue;
       uint32_t x[WORDS];
       if constexpr (RO && IBFS_BU_NC) ld_status_nc<WORDS>(gb.last + (size_t)u * WORDS, x);
       else ld_status<WORDS>(gb.last + (size_t)u * WORDS, x);
@@ -869,7 +1075,8 @@ __device__ __forceinline__ void ld_nbr(const uint32_t* last, const uint32_t* s_h
 template <int WORDS, bool FUSED = false, bool RO = FUSED, int HK = 0>
 __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
                          const uint32_t* fmask_g, int32_t* hq_cnt, const Team& t,
-                         Par* par = nullptr, int n_b = 0, bool depth_ok = true) {
+                         Par* par = nullptr, int n_b = 0, bool depth_ok = true,
+                         bool filt = false) {
   constexpr bool NC = RO && IBFS_BU_NC;
   // Hub status cache (HK > 0, passes that run as their own kernel: `last` is
   // not written while they run).  The degree order puts the highest-degree vertices at
@@ -931,7 +1138,7 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
         for (int k = 0; k < WORDS; k++) x[k] = 0;
         if (e + lane < e_lim) {
           const int32_t u = p.col[e + lane];
-          if (!p.bu_filter || ((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u))
+          if (!filt || in_front<RO>(front, u))
             ld_nbr<WORDS, HK, NC>(gb.last, s_hub, hk, u, x);
         }
         miss = false;
@@ -1021,14 +1228,23 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
     }
     need = need && valid && (b1 > b0);
     const bool small = need && (b1 - b0) <= p.but;
-    if (small) {
+    // Every vertex that needs bits scans on its own lane first: a small one
+    // its whole list, a big one only its first kBuPeek steps -- its
+    // highest-degree neighbours, which in the degree order usually cover
+    // the frontier bits already.  Only big vertices still missing bits go on
+    // to the warp scan below, which takes them one at a time.
+    bool covered = false;
+    long long e_big = b0;  // where a big vertex's warp scan starts
+    if (need) {
       // kBuStep neighbours in flight per step; with col_vec their ids come as
       // aligned 16-byte vectors (col is padded by 4 entries at its end, and
       // a vector is only read when it starts before b1)
       constexpr int S = kBuStep;
       const int4* col4 = reinterpret_cast<const int4*>(p.col);
       const long long a0 = p.col_vec ? (b0 & ~3LL) : b0;
-      for (long long a = a0; a < b1; a += S) {
+      const long long a_end = small ? b1 : min(b1, a0 + (long long)kBuPeek * S);
+      if (!small) e_big = max(b0, a_end);
+      for (long long a = a0; a < a_end; a += S) {
         int32_t u[S];
         if (p.col_vec) {
 #pragma unroll
@@ -1045,7 +1261,7 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
 #pragma unroll
         for (int i = 0; i < S; i++) {
           const bool in = (a + i >= b0) && (a + i < b1);
-          f[i] = in && (!p.bu_filter || ((__ldcg(front + (u[i] >> 5)) >> (u[i] & 31)) & 1u));
+          f[i] = in && (!filt || in_front<RO>(front, u[i]));
         }
         uint32_t x[S][WORDS];
 #pragma unroll
@@ -1064,30 +1280,35 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
           for (int i = 0; i < S; i++) acc[k] |= x[i][k];
           miss |= (fm[k] & ~acc[k]) != 0u;
         }
-        if (!miss) break;
+        if (!miss) {
+          covered = true;
+          break;
+        }
       }
     }
     bool deferred = false;  // this lane's vertex left chunks to bu_defer_phase
-    uint32_t big = __ballot_sync(0xFFFFFFFFu, need && !small);
+    uint32_t big = __ballot_sync(0xFFFFFFFFu, need && !small && !covered);
     while (big) {
       const int j = __ffs(big) - 1;
       big &= big - 1;
       const long long e0 = __shfl_sync(0xFFFFFFFFu, b0, j);
       const long long e1 = __shfl_sync(0xFFFFFFFFu, b1, j);
+      const long long es = __shfl_sync(0xFFFFFFFFu, e_big, j);
       uint32_t a[WORDS];
 #pragma unroll
       for (int k = 0; k < WORDS; k++) a[k] = __shfl_sync(0xFFFFFFFFu, acc[k], j);
       // a warp scans at most hub_t neighbours; the rest of a hub that is
       // still missing frontier bits is deferred to bu_defer_phase
+      // (the limit counts from the list's start, as bu_defer_phase does)
       const long long e_lim = (e1 - e0 > p.hub_t) ? e0 + p.hub_t : e1;
       bool miss = true;
-      for (long long e = e0; e < e_lim; e += 32) {
+      for (long long e = es; e < e_lim; e += 32) {
         uint32_t x[WORDS];
 #pragma unroll
         for (int k = 0; k < WORDS; k++) x[k] = 0;
         if (e + lane < e_lim) {
           const int32_t u = p.col[e + lane];
-          if (!p.bu_filter || ((__ldcg(front + (u >> 5)) >> (u & 31)) & 1u))
+          if (!filt || in_front<RO>(front, u))
             ld_nbr<WORDS, HK, NC>(gb.last, s_hub, hk, u, x);
         }
         miss = false;

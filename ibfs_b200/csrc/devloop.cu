@@ -278,7 +278,8 @@ template <int WORDS>
 __global__ void __launch_bounds__(512) k_dl_td(Params p, int g, CondH, CondH) {
   const GroupBufs gb = dl_bufs(p, g);
   const int level = gb.ctl->ls.level;
-  td_phase<WORDS>(p, gb, level, gb.ctl->qc[level & 1], make_team(blockIdx.x, gridDim.x));
+  td_phase<WORDS, true>(p, gb, level, gb.ctl->qc[level & 1],
+                                      make_team(blockIdx.x, gridDim.x));
 }
 
 template <int WORDS>
@@ -287,14 +288,15 @@ __global__ void DL_BU_BOUNDS k_dl_bu(Params p, int g, CondH, CondH) {
   const LoopState& ls = gb.ctl->ls;
   const int level = ls.level;
   const Team t = make_team(blockIdx.x, gridDim.x);
+  const bool filt = bu_filter_level(p.bu_filter, gb.ctl->par[(level - 1) & 1].changed, p.V);
   if (IBFS_DL_FUSED_BU) {
     bu_phase<WORDS, true, true, IBFS_BU_HUB_BYTES / (4 * WORDS)>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
                           &gb.ctl->par[level & 1].hq_cnt, t, &gb.ctl->par[level & 1],
-                          dl_batch_size(p, ls, ls.batch), level <= depth_limit(p.db));
+                          dl_batch_size(p, ls, ls.batch), level <= depth_limit(p.db), filt);
   } else {
     zero_plane_if_first(p, gb, level, t);
     bu_phase<WORDS, false, true>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
-                                 &gb.ctl->par[level & 1].hq_cnt, t);
+                                 &gb.ctl->par[level & 1].hq_cnt, t, nullptr, 0, true, filt);
   }
 }
 
@@ -315,7 +317,9 @@ __global__ void __launch_bounds__(512) k_dl_bu_defer(Params p, int g, CondH, Con
   const int level = gb.ctl->ls.level;
   if (gb.ctl->par[level & 1].hq_cnt == 0) return;  // uniform: nothing deferred
   bu_defer_phase<WORDS, true>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
-                              &gb.ctl->par[level & 1].hq_cnt, make_team(blockIdx.x, gridDim.x));
+                              &gb.ctl->par[level & 1].hq_cnt, make_team(blockIdx.x, gridDim.x),
+                              bu_filter_level(p.bu_filter, gb.ctl->par[(level - 1) & 1].changed,
+                                              p.V));
 }
 
 // threads per CTA and CTAs per SM of the output pass (R-MAT scale 24, one

@@ -62,21 +62,25 @@ __global__ void __launch_bounds__(512) k_qbuild(Params p, GroupBufs gb, int leve
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_td(Params p, GroupBufs gb, int level) {
   const Team t = make_team(blockIdx.x, gridDim.x);
-  td_phase<WORDS>(p, gb, level, gb.ctl->qc[level & 1], t);
+  td_phase<WORDS, true>(p, gb, level, gb.ctl->qc[level & 1], t);
 }
 
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_bu(Params p, GroupBufs gb, int level) {
   const Team t = make_team(blockIdx.x, gridDim.x);
   bu_phase<WORDS, false, true>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
-                               &gb.ctl->par[level & 1].hq_cnt, t);
+                               &gb.ctl->par[level & 1].hq_cnt, t, nullptr, 0, true,
+                               bu_filter_level(p.bu_filter, gb.ctl->par[(level - 1) & 1].changed,
+                                               p.V));
 }
 
 template <int WORDS>
 __global__ void __launch_bounds__(512) k_bu_defer(Params p, GroupBufs gb, int level) {
   const Team t = make_team(blockIdx.x, gridDim.x);
   bu_defer_phase<WORDS, true>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
-                              &gb.ctl->par[level & 1].hq_cnt, t);
+                              &gb.ctl->par[level & 1].hq_cnt, t,
+                              bu_filter_level(p.bu_filter, gb.ctl->par[(level - 1) & 1].changed,
+                                              p.V));
 }
 
 template <int WORDS>
@@ -366,7 +370,8 @@ void fill_graph_params(const ibfs_graph* g, const ibfs_opts& o, int words, int t
   p.timeout_ns = (unsigned long long)(o.timeout_ms ? o.timeout_ms : 10000) * 1000000ull;
   p.withhold = o.debug_withhold;
   p.hub_t = kHubScan;
-  p.bu_filter = o.bu_filter > 0 ? 1 : 0;
+  p.bu_filter = o.bu_filter > 0 ? 1 : o.bu_filter == 0 ? 0 : -1;
+  p.td_stage = o.td_stage > 0 ? 1 : 0;
   p.col_vec = 1;
   p.vmap = g->vmap.as<int32_t>();
   // Degrees are non-increasing in the internal order: the vertices above the
@@ -476,7 +481,7 @@ extern "C" void ibfs_opts_default(ibfs_opts* o) {
   o->max_levels = 0;
   o->debug_withhold = 0;
   o->occupancy = 0;
-  o->bu_filter = -1;  // default: off (measured faster on B200)
+  o->bu_filter = -1;  // default: per level, on when the previous frontier is small
   o->bu_thread_max = 32;
 }
 

@@ -109,12 +109,14 @@ __global__ void __launch_bounds__(THREADS, MINB) persistent_kernel(Params p) {
         td_phase<WORDS>(p, gb, level, ctl->qc[level & 1], t);
       } else {
         bu++;
+        const bool filt =
+            bu_filter_level(p.bu_filter, __ldcg(&ctl->par[(level - 1) & 1].changed), p.V);
         bu_phase<WORDS>(p, gb, level, ctl->par[(level - 1) & 1].fmask,
-                        &ctl->par[level & 1].hq_cnt, t);
+                        &ctl->par[level & 1].hq_cnt, t, nullptr, 0, true, filt);
         BARRIER();
         if (__ldcg(&ctl->par[level & 1].hq_cnt) > 0) {  // same value in every CTA
           bu_defer_phase<WORDS>(p, gb, level, ctl->par[(level - 1) & 1].fmask,
-                                &ctl->par[level & 1].hq_cnt, t);
+                                &ctl->par[level & 1].hq_cnt, t, filt);
           BARRIER();
         }
         if (lead) t_mid = global_ns();

@@ -109,12 +109,17 @@ typedef struct ibfs_opts {
                               0: 512 threads x 2 CTAs (64 regs), 1: 256 x 6 (42),
                               2: 256 x 8 (32), 3: 512 x 1 (128)                 */
     int32_t bu_filter;     /* bottom-up reads a neighbour's status only when the
-                              previous frontier bitmap has it: 1 on, 0 or -1 off
-                              (the default: the bitmap lookup costs more than the
-                              status reads it saves)                              */
+                              previous frontier bitmap has it (exact: no other
+                              neighbour can add a bit): 1 on every level, 0 off,
+                              -1 (default) on levels whose previous frontier
+                              holds fewer than V/16 vertices                      */
     int32_t bu_thread_max; /* bottom-up: vertices of degree <= this scan alone, one
                               thread each; above it a warp scans (0: 32)          */
-    int32_t reserved[4];
+    int32_t td_stage;      /* 1: top-down stages each large vertex's adjacency
+                              chunk in shared memory by double-buffered bulk
+                              (TMA) copies (plain and device-loop schedules);
+                              0 (default): reads the chunk directly              */
+    int32_t reserved[3];
 } ibfs_opts;
 
 typedef struct ibfs_level_rec {

@@ -291,3 +291,27 @@ def test_internal_vertex_order():
     for new in range(0, V, 37):
         old = order[new]
         assert np.array_equal(nc[nb[new]:nb[new + 1]], np.sort(nm[col[beg[old]:beg[old + 1]]]))
+
+
+@pytest.mark.parametrize("bu_filter", [0, 1, -1])
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("kind", ["rmat13", "grid", "chunglu"])
+def test_bottom_up_frontier_filter(kind, mode, bu_filter):
+    """The frontier filter (skip neighbours outside the previous frontier)
+    is exact: off, on every bottom-up level, and per level (the default)."""
+    beg, col, g = graph(kind)
+    src = ib.sample_sources(beg, col, 128, seed=7)
+    run_and_check(beg, col, g, src, width=128, mode=mode, switch_level=1, bu_filter=bu_filter)
+
+
+@pytest.mark.parametrize("thresholds", [(32, 512), (1, 1)])
+@pytest.mark.parametrize("mode", [ib.MODE_PLAIN, ib.MODE_DEVICE_LOOP])
+@pytest.mark.parametrize("kind", ["rmat13", "chunglu"])
+def test_top_down_staged_chunks(kind, mode, thresholds):
+    """Large vertices' adjacency chunks staged in shared memory by bulk
+    copies give the same depths; thresholds (1, 1) send every frontier
+    vertex through the chunked path."""
+    beg, col, g = graph(kind)
+    src = ib.sample_sources(beg, col, 128, seed=9)
+    run_and_check(beg, col, g, src, width=128, mode=mode, switch_level=2, td_stage=1,
+                  sml_shed=thresholds[0], lrg_shed=thresholds[1])
