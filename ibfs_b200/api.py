@@ -44,7 +44,7 @@ class Opts(C.Structure):
         ("ctas_per_sm", C.c_int32), ("use_graph", C.c_int32), ("timeout_ms", C.c_int32),
         ("max_levels", C.c_int32), ("debug_withhold", C.c_int32), ("occupancy", C.c_int32),
         ("bu_filter", C.c_int32), ("bu_thread_max", C.c_int32), ("td_stage", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("sparse_push", C.c_int32), ("reserved", C.c_int32 * 2),
     ]
 
 

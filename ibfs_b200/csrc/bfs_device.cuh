@@ -47,7 +47,10 @@ struct Par {
   uint32_t fmask[kMaxWords];   // OR of all new bits (sources still expanding)
   int32_t range_err;           // a level did not fit the depth type
   int32_t hq_cnt;              // deferred bottom-up hub chunks of this level
-  int32_t pad[2];
+  int32_t pq_cnt;              // queued sparse-source push chunks of this level
+  int32_t pad;
+  uint32_t scnt[kMaxWords * 32];  // per source: vertices it reached at the
+                                  // previous level (sparse_count_phase)
 };
 
 // State of the level loop when it runs as kernels inside a CUDA graph (the
@@ -65,6 +68,9 @@ struct LoopState {
   int32_t flip;       // 1: the status "last" lives in GroupBufs::curr and vice versa
   int32_t sync;       // the next top-down level first copies new statuses over old ones
   int32_t nb;         // sources of `batch`
+  uint32_t smask[kMaxWords];  // bottom-up level: sources pushed top-down instead
+  int32_t sparse_try;         // this bottom-up level follows a top-down one: count
+                              // the sources' frontiers and pick the sparse ones
   unsigned long long m_u, teps, prev_changed;
   unsigned long long t_lvl, t_mid;  // %globaltimer at the level start / inspect start
 };
@@ -135,6 +141,9 @@ struct Params {
   int vec_sm;   // source-major rows allow vector stores of this many bytes: 16 (V % 16
                 // == 0, 16-byte aligned base), 4 (V % 4 == 0, 4-byte aligned) or 0
   int td_stage;     // top-down stages large vertices' chunks by bulk copies
+  int sparse_div;   // device loop: a bottom-up level pushes, top-down, the sources
+                    // whose previous frontier is below 1/sparse_div of the average
+                    // (0: off; see sparse_count_phase)
   int bu_filter;    // bottom-up skips neighbours outside the previous frontier:
                     // 1 always, 0 never, -1 on levels whose previous frontier
                     // is small (bu_filter_level)
@@ -387,6 +396,20 @@ __device__ __forceinline__ void cta_or_u32(uint32_t* dst, uint32_t x) {
   }
 }
 
+// Per-source counts of a level's new bits, for the sparse-source decision:
+// shared-memory counters per CTA (every thread calls scnt_begin and
+// scnt_flush), one atomic add per counted (vertex, source) pair.
+__device__ __forceinline__ void scnt_begin(uint32_t* s_cnt) {
+  for (int i = threadIdx.x; i < kMaxWords * 32; i += blockDim.x) s_cnt[i] = 0u;
+  __syncthreads();
+}
+template <int WORDS>
+__device__ __forceinline__ void scnt_flush(const uint32_t* s_cnt, Par* par) {
+  __syncthreads();
+  for (int i = threadIdx.x; i < WORDS * 32; i += blockDim.x)
+    if (s_cnt[i]) atomicAdd(&par->scnt[i], s_cnt[i]);
+}
+
 __device__ __forceinline__ void zero_words(uint32_t* p, long long nwords, const Team& t) {
   // nwords is a multiple of 4 and p 16-byte aligned (allocation padding)
   uint4* q = reinterpret_cast<uint4*>(p);
@@ -454,8 +477,9 @@ __device__ __forceinline__ void inspect_vertex(const Params& p, const GroupBufs&
                                                const uint32_t (&full)[WORDS], uint32_t (&fm)[WORDS],
                                                unsigned long long& mf, unsigned long long& cnt,
                                                unsigned long long& cdeg,
-                                               unsigned long long& teps) {
-  uint32_t c[WORDS], l[WORDS], nb[WORDS];
+                                               unsigned long long& teps,
+                                               uint32_t (&nb)[WORDS]) {
+  uint32_t c[WORDS], l[WORDS];
   ld_status<WORDS>(gb.curr + (size_t)v * WORDS, c);
   ld_status<WORDS>(gb.last + (size_t)v * WORDS, l);
   bool comp = true;
@@ -535,13 +559,14 @@ __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par, in
   // bottom-up merges into it with atomics
   zero_words(chg_at(gb, p, level + 1), p.chg_stride, t);
   const int lane = t.lane;
+  uint32_t nbx[WORDS];  // the new bits of the vertex a lane inspected (unused here)
   if (LEAN && dense) {
     for (long long w = t.warp; w < p.nchg; w += t.nwarps) {
       const uint32_t bits = __ldcg(chg + w);
       if (!bits) continue;
       const long long v = w * 32 + lane;
       if ((bits >> lane) & 1u)
-        inspect_vertex<WORDS>(p, gb, v, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
+        inspect_vertex<WORDS>(p, gb, v, level, depth_ok, full, fm, mf, cnt, cdeg, teps, nbx);
     }
   } else if (LEAN) {
     const long long nblk = (p.nchg + 127) / 128;
@@ -557,13 +582,13 @@ __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par, in
         const uint32_t b3 = __shfl_sync(0xFFFFFFFFu, q4.w, src);
         const long long w0 = blk * 128 + src * 4;
         if ((b0 >> lane) & 1u)
-          inspect_vertex<WORDS>(p, gb, (w0 + 0) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
+          inspect_vertex<WORDS>(p, gb, (w0 + 0) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps, nbx);
         if ((b1 >> lane) & 1u)
-          inspect_vertex<WORDS>(p, gb, (w0 + 1) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
+          inspect_vertex<WORDS>(p, gb, (w0 + 1) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps, nbx);
         if ((b2 >> lane) & 1u)
-          inspect_vertex<WORDS>(p, gb, (w0 + 2) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
+          inspect_vertex<WORDS>(p, gb, (w0 + 2) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps, nbx);
         if ((b3 >> lane) & 1u)
-          inspect_vertex<WORDS>(p, gb, (w0 + 3) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
+          inspect_vertex<WORDS>(p, gb, (w0 + 3) * 32 + lane, level, depth_ok, full, fm, mf, cnt, cdeg, teps, nbx);
       }
     }
   } else {
@@ -594,7 +619,7 @@ __device__ void inspect_phase(const Params& p, const GroupBufs& gb, Par* par, in
       if (r < total) {
         const int bit = (int)__fns(w, 0u, r - e + 1);
         const long long v = (c * 32 + lo) * 32 + bit;
-        inspect_vertex<WORDS>(p, gb, v, level, depth_ok, full, fm, mf, cnt, cdeg, teps);
+        inspect_vertex<WORDS>(p, gb, v, level, depth_ok, full, fm, mf, cnt, cdeg, teps, nbx);
       }
     }
   }
@@ -948,13 +973,13 @@ __device__ void td_phase(const Params& p, const GroupBufs& gb, int level, const 
 template <int WORDS, bool RO = false>
 __device__ void bu_defer_phase(const Params& p, const GroupBufs& gb, int level,
                                const uint32_t* fmask_g, const int32_t* hq_cnt, const Team& t,
-                               bool filt = false) {
+                               bool filt = false, const uint32_t* smask = nullptr) {
   __shared__ uint32_t s_acc[32][kMaxWords];
   __shared__ uint32_t s_cur[kMaxWords];
   __shared__ int s_skip;
   uint32_t fm[WORDS];
 #pragma unroll
-  for (int k = 0; k < WORDS; k++) fm[k] = __ldcg(fmask_g + k);
+  for (int k = 0; k < WORDS; k++) fm[k] = __ldcg(fmask_g + k) & (smask ? ~__ldcg(smask + k) : ~0u);
   const uint32_t* front = chg_at(gb, p, level - 1);
   uint32_t* out = chg_at(gb, p, level);
   const int n = __ldcg(hq_cnt);
@@ -1072,11 +1097,13 @@ __device__ __forceinline__ void ld_nbr(const uint32_t* last, const uint32_t* s_h
   else ld_status<WORDS>(last + (size_t)u * WORDS, x);
 }
 
+// smask (device loop, sparse-source levels): bits pushed top-down after this
+// pass (push_queue_phase / push_run_phase); the scan's early exit ignores them.
 template <int WORDS, bool FUSED = false, bool RO = FUSED, int HK = 0>
 __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
                          const uint32_t* fmask_g, int32_t* hq_cnt, const Team& t,
                          Par* par = nullptr, int n_b = 0, bool depth_ok = true,
-                         bool filt = false) {
+                         bool filt = false, const uint32_t* smask = nullptr) {
   constexpr bool NC = RO && IBFS_BU_NC;
   // Hub status cache (HK > 0, passes that run as their own kernel: `last` is
   // not written while they run).  The degree order puts the highest-degree vertices at
@@ -1093,7 +1120,7 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
   }
   uint32_t fm[WORDS];
 #pragma unroll
-  for (int k = 0; k < WORDS; k++) fm[k] = __ldcg(fmask_g + k);
+  for (int k = 0; k < WORDS; k++) fm[k] = __ldcg(fmask_g + k) & (smask ? ~__ldcg(smask + k) : ~0u);
   const uint32_t* front = chg_at(gb, p, level - 1);
   uint32_t* out = chg_at(gb, p, level);
   const int lane = t.lane;
@@ -1403,10 +1430,13 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
 // scan was deferred (one entry per hub: chunk 0), from their final status
 // in `curr` and the previous one in `last`; and the level+1 bitmap cleared
 // for the next expand (what inspect_phase does on other levels).
+// keep_next: a sparse-source push follows and still reads the level-(L-1)
+// bitmap, which is the same buffer as level L+1's (level parity); the push
+// kernel's successor clears it then.
 template <int WORDS>
 __device__ void bu_hub_epilogue(const Params& p, const GroupBufs& gb, Par* par, int n_b,
-                                int level, bool depth_ok, const Team& t) {
-  zero_words(chg_at(gb, p, level + 1), p.chg_stride, t);
+                                int level, bool depth_ok, const Team& t, bool keep_next = false) {
+  if (!keep_next) zero_words(chg_at(gb, p, level + 1), p.chg_stride, t);
   uint32_t full[WORDS], fm[WORDS];
 #pragma unroll
   for (int k = 0; k < WORDS; k++) {
@@ -1461,6 +1491,246 @@ __device__ void bu_hub_epilogue(const Params& p, const GroupBufs& gb, Par* par, 
   cta_add_u64(&par->teps, teps);
 #pragma unroll
   for (int k = 0; k < WORDS; k++) cta_or_u32(&par->fmask[k], fm[k]);
+}
+
+// ---------------------------------------------------------------------------
+// Sparse sources (device loop, a bottom-up level L that follows a top-down
+// level).  A bottom-up scan stops once a vertex holds every bit of the
+// previous frontier.  A source whose level-(L-1) frontier holds only a
+// handful of vertices (it started far from the hubs) has not reached most
+// vertices yet, so with its bit in the mask almost no vertex can stop early
+// and most scan their whole neighbour lists.  So at such a level:
+//   sparse_count_phase  counts every source's level-(L-1) frontier;
+//   (k_dl_sparse_decide) the sources below 1/sparse_div of the average go
+//                       into LoopState::smask, and the bottom-up pass's
+//                       early exit ignores their bits;
+//   push_queue_phase /  after the pass (and its deferred hubs), those bits
+//   push_run_phase      are delivered exactly as a top-down level would:
+//                       every vertex that gained a sparse bit at level L-1
+//                       pushes it to all its neighbours -- a warp per small
+//                       vertex, 2048-edge chunks spread over all CTAs for a
+//                       vertex above the large-queue threshold (a hub can be
+//                       in a sparse source's frontier).
+// Each push takes its new bits from the atomic OR's old value, so the
+// level's edge count, its depth planes (OR reductions: other pushes may hit
+// the same vertex) and fmask stay exact; the changed count, the frontier-edge
+// sum and the completed-degree sum (which only steer the direction choice)
+// count a vertex when a push is the first change to it at this level.  The
+// result is the BFS of every source: a bit reaches each vertex at its
+// distance either way.
+// ---------------------------------------------------------------------------
+// The bits of `mask` that v gained at level L-1 (`last` holds the statuses
+// after level L-1; a bit's depth is L-1 when the planes spell L-1: the planes
+// of bits already in `last` no longer change).
+template <int WORDS>
+__device__ __forceinline__ bool gained_at(const Params& p, const GroupBufs& gb, long long v,
+                                          int lp, const uint32_t (&mask)[WORDS],
+                                          uint32_t (&P)[WORDS]) {
+  ld_status<WORDS>(gb.last + (size_t)v * WORDS, P);
+  bool has = false;
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) {
+    P[k] &= mask[k];
+    has |= P[k] != 0u;
+  }
+  if (!has) return false;
+  const int np = planes_for(lp);
+  for (int b = 0; b < np; b++) {
+    uint32_t x[WORDS];
+    ld_status<WORDS>(gb.planes + (size_t)b * p.plane_stride + (size_t)v * WORDS, x);
+    const bool one = (lp >> b) & 1;
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) P[k] &= one ? x[k] : ~x[k];
+  }
+  has = false;
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) has |= P[k] != 0u;
+  return has;
+}
+
+template <int WORDS>
+__device__ void sparse_count_phase(const Params& p, const GroupBufs& gb, Par* par, int level,
+                                   const Team& t) {
+  __shared__ uint32_t s_scnt[kMaxWords * 32];
+  scnt_begin(s_scnt);
+  uint32_t all[WORDS];
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) all[k] = 0xFFFFFFFFu;
+  const uint32_t* front = chg_at(gb, p, level - 1);
+  for (long long v = t.tid; v < p.V; v += t.nthreads) {
+    if (!((__ldcg(front + (v >> 5)) >> (v & 31)) & 1u)) continue;
+    uint32_t P[WORDS];
+    if (!gained_at<WORDS>(p, gb, v, level - 1, all, P)) continue;
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) {
+      uint32_t r = P[k];
+      while (r) {
+        atomicAdd(&s_scnt[k * 32 + __ffs(r) - 1], 1u);
+        r &= r - 1;
+      }
+    }
+  }
+  scnt_flush<WORDS>(s_scnt, par);
+}
+
+struct PushAcc {
+  unsigned long long mf = 0, cnt = 0, cdeg = 0, teps = 0;
+  uint32_t fm[kMaxWords] = {0, 0, 0, 0, 0, 0, 0, 0};
+  bool range = false;
+};
+
+// One pushed edge: OR the bits P into u's status and account for the ones
+// that were new (see above).
+template <int WORDS>
+__device__ __forceinline__ void push_edge(const Params& p, const GroupBufs& gb, uint32_t* out,
+                                          int level, bool depth_ok, const uint32_t (&full)[WORDS],
+                                          int32_t u, const uint32_t (&P)[WORDS], PushAcc& acc) {
+  uint32_t s[WORDS];
+  ld_status<WORDS>(gb.curr + (size_t)u * WORDS, s);
+  bool need = false;
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) need |= (P[k] & ~s[k]) != 0u;
+  if (!need) return;
+  uint32_t old[WORDS], nb[WORDS];
+  if constexpr (WORDS == 1) {
+    old[0] = atomicOr(gb.curr + u, P[0]);
+  } else {
+    unsigned long long* q = reinterpret_cast<unsigned long long*>(gb.curr + (size_t)u * WORDS);
+#pragma unroll
+    for (int k = 0; k < WORDS / 2; k++) {
+      const unsigned long long pw = ((unsigned long long)P[2 * k + 1] << 32) | P[2 * k];
+      const unsigned long long o =
+          pw ? atomicOr(q + k, pw) : (((unsigned long long)s[2 * k + 1] << 32) | s[2 * k]);
+      old[2 * k] = (uint32_t)o;
+      old[2 * k + 1] = (uint32_t)(o >> 32);
+    }
+  }
+  bool any = false;
+  uint32_t pop = 0;
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) {
+    nb[k] = P[k] & ~old[k];
+    any |= nb[k] != 0u;
+    pop += __popc(nb[k]);
+  }
+  if (!any) return;
+  uint32_t l[WORDS];
+  ld_status<WORDS>(gb.last + (size_t)u * WORDS, l);
+  bool first = true, was_full = true, now_full = true;
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) {
+    first = first && (old[k] & ~l[k]) == 0u;
+    was_full = was_full && old[k] == full[k];
+    now_full = now_full && (old[k] | nb[k]) == full[k];
+    acc.fm[k] |= nb[k];
+  }
+  const unsigned long long deg = (unsigned long long)(p.beg[u + 1] - p.beg[u]);
+  acc.teps += deg * pop;
+  if (first) {
+    acc.cnt += 1;
+    acc.mf += deg;
+  }
+  if (now_full && !was_full) acc.cdeg += deg;
+  red_or_u32(out + (u >> 5), 1u << (u & 31));
+  if (!depth_ok) {
+    acc.range = true;
+    return;
+  }
+  unsigned rest = (unsigned)level;
+  while (rest) {
+    const int b = __ffs(rest) - 1;
+    rest &= rest - 1;
+    uint32_t* q = gb.planes + (size_t)b * p.plane_stride + (size_t)u * WORDS;
+#pragma unroll
+    for (int k = 0; k < WORDS; k++)
+      if (nb[k]) red_or_u32(q + k, nb[k]);
+  }
+}
+
+template <int WORDS>
+__device__ __forceinline__ void push_acc_flush(const PushAcc& acc, Par* par) {
+  if (acc.range) par->range_err = 1;
+  cta_add_u64(&par->changed, acc.cnt);
+  cta_add_u64(&par->mf, acc.mf);
+  cta_add_u64(&par->cdeg, acc.cdeg);
+  cta_add_u64(&par->teps, acc.teps);
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) cta_or_u32(&par->fmask[k], acc.fm[k]);
+}
+
+template <int WORDS>
+__device__ void push_queue_phase(const Params& p, const GroupBufs& gb, Par* par, int n_b,
+                                 int level, bool depth_ok, const uint32_t* smask,
+                                 const Team& t) {
+  uint32_t sm[WORDS], full[WORDS];
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) {
+    sm[k] = __ldcg(smask + k);
+    full[k] = full_word(n_b, k);
+  }
+  const uint32_t* front = chg_at(gb, p, level - 1);
+  uint32_t* out = chg_at(gb, p, level);
+  PushAcc acc;
+  const int lane = t.lane;
+  for (long long w = t.warp; w < p.nchg; w += t.nwarps) {
+    const uint32_t bits = __ldcg(front + w);
+    if (!bits) continue;  // uniform
+    const long long v0 = w * 32 + lane;
+    uint32_t P[WORDS];
+    bool has = false;
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) P[k] = 0u;
+    long long deg = 0;
+    if ((bits >> lane) & 1u) {
+      has = gained_at<WORDS>(p, gb, v0, level - 1, sm, P);
+      if (has) deg = p.beg[v0 + 1] - p.beg[v0];
+    }
+    // a vertex above the large-queue threshold goes to the chunk queue
+    if (has && deg > p.lrg) {
+      const int nch = (int)((deg + p.chunk - 1) / p.chunk);
+      const int base0 = atomicAdd(&par->pq_cnt, nch);
+      for (int c = 0; c < nch; c++) gb.ql[base0 + c] = make_int2((int)v0, c);
+      has = false;
+    }
+    uint32_t pushers = __ballot_sync(0xFFFFFFFFu, has);
+    while (pushers) {
+      const int j = __ffs(pushers) - 1;
+      pushers &= pushers - 1;
+      uint32_t Pj[WORDS];
+#pragma unroll
+      for (int k = 0; k < WORDS; k++) Pj[k] = __shfl_sync(0xFFFFFFFFu, P[k], j);
+      const long long v = w * 32 + j;
+      const long long e1 = p.beg[v + 1];
+      for (long long e = p.beg[v] + lane; e < e1; e += 32)
+        push_edge<WORDS>(p, gb, out, level, depth_ok, full, __ldg(p.col + e), Pj, acc);
+    }
+  }
+  push_acc_flush<WORDS>(acc, par);
+}
+
+template <int WORDS>
+__device__ void push_run_phase(const Params& p, const GroupBufs& gb, Par* par, int n_b,
+                               int level, bool depth_ok, const uint32_t* smask, const Team& t) {
+  uint32_t sm[WORDS], full[WORDS];
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) {
+    sm[k] = __ldcg(smask + k);
+    full[k] = full_word(n_b, k);
+  }
+  uint32_t* out = chg_at(gb, p, level);
+  PushAcc acc;
+  const int n = __ldcg(&par->pq_cnt);
+  for (int c = t.block; c < n; c += t.nblocks) {
+    const int2 d = gb.ql[c];
+    uint32_t P[WORDS];
+    (void)gained_at<WORDS>(p, gb, d.x, level - 1, sm, P);
+    const long long e_end = p.beg[d.x + 1];
+    const long long b0 = p.beg[d.x] + (long long)d.y * p.chunk;
+    const long long b1 = min(e_end, b0 + (long long)p.chunk);
+    for (long long e = b0 + threadIdx.x; e < b1; e += blockDim.x)
+      push_edge<WORDS>(p, gb, out, level, depth_ok, full, __ldg(p.col + e), P, acc);
+  }
+  push_acc_flush<WORDS>(acc, par);
 }
 
 // ---------------------------------------------------------------------------

@@ -36,6 +36,15 @@
 #ifndef IBFS_DL_INSPECT_MINB
 #define IBFS_DL_INSPECT_MINB 3
 #endif
+// CTAs per SM the top-down kernel must fit (0: left to the compiler)
+#ifndef IBFS_DL_TD_MINB
+#define IBFS_DL_TD_MINB 0
+#endif
+#if IBFS_DL_TD_MINB > 0
+#define DL_TD_BOUNDS __launch_bounds__(512, IBFS_DL_TD_MINB)
+#else
+#define DL_TD_BOUNDS __launch_bounds__(512)
+#endif
 #if IBFS_DL_BU_MINB > 0
 #define DL_BU_BOUNDS __launch_bounds__(IBFS_DL_BU_THREADS, IBFS_DL_BU_MINB)
 #else
@@ -195,6 +204,8 @@ __global__ void __launch_bounds__(512) k_dl_batch_init(Params p, int g, CondH h_
     ls.prev_changed = 0;
     ls.flip = 0;
     ls.sync = 0;
+    for (int k = 0; k < kMaxWords; k++) ls.smask[k] = 0u;
+    ls.sparse_try = 0;
     ls.t_lvl = ls.t_mid = global_ns();
     cudaGraphSetConditional(h_level, 1u);
   }
@@ -242,6 +253,11 @@ __global__ void k_dl_decide(Params p, int g, CondH h_level, CondH h_dir) {
   const int nd = choose_dir(level + 1, ls.dir, p.switch_level, p.alpha, p.beta, changed,
                             ls.prev_changed, mf, ls.m_u, p.V);
   ls.prev_changed = changed;
+  // A bottom-up level right after a top-down one looks for sparse sources
+  // (k_dl_sparse_count / k_dl_sparse_decide fill smask before its pass)
+#pragma unroll
+  for (int k = 0; k < kMaxWords; k++) ls.smask[k] = 0u;
+  ls.sparse_try = (!stop && nd == kDirBU && ls.dir == kDirTD && level > 0 && p.sparse_div > 0) ? 1 : 0;
   const unsigned long long t_now = global_ns();
   if (level < p.lrec_cap) {
     LevelRec r;
@@ -275,7 +291,7 @@ __global__ void __launch_bounds__(512) k_dl_qbuild(Params p, int g, CondH, CondH
 }
 
 template <int WORDS>
-__global__ void __launch_bounds__(512) k_dl_td(Params p, int g, CondH, CondH) {
+__global__ void DL_TD_BOUNDS k_dl_td(Params p, int g, CondH, CondH) {
   const GroupBufs gb = dl_bufs(p, g);
   const int level = gb.ctl->ls.level;
   td_phase<WORDS, true>(p, gb, level, gb.ctl->qc[level & 1],
@@ -292,7 +308,8 @@ __global__ void DL_BU_BOUNDS k_dl_bu(Params p, int g, CondH, CondH) {
   if (IBFS_DL_FUSED_BU) {
     bu_phase<WORDS, true, true, IBFS_BU_HUB_BYTES / (4 * WORDS)>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
                           &gb.ctl->par[level & 1].hq_cnt, t, &gb.ctl->par[level & 1],
-                          dl_batch_size(p, ls, ls.batch), level <= depth_limit(p.db), filt);
+                          dl_batch_size(p, ls, ls.batch), level <= depth_limit(p.db), filt,
+                          ls.smask);
   } else {
     zero_plane_if_first(p, gb, level, t);
     bu_phase<WORDS, false, true>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
@@ -307,8 +324,9 @@ __global__ void __launch_bounds__(512) k_dl_bu_hubs(Params p, int g, CondH, Cond
   Ctl* ctl = gb.ctl;
   const int b = ctl->ls.batch, level = ctl->ls.level;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ls.t_mid = global_ns();
+  const bool sparse = dl_sparse(ctl->ls, WORDS);
   bu_hub_epilogue<WORDS>(p, gb, &ctl->par[level & 1], dl_batch_size(p, ctl->ls, b), level,
-                         level <= depth_limit(p.db), make_team(blockIdx.x, gridDim.x));
+                         level <= depth_limit(p.db), make_team(blockIdx.x, gridDim.x), sparse);
 }
 
 template <int WORDS>
@@ -319,7 +337,83 @@ __global__ void __launch_bounds__(512) k_dl_bu_defer(Params p, int g, CondH, Con
   bu_defer_phase<WORDS, true>(p, gb, level, gb.ctl->par[(level - 1) & 1].fmask,
                               &gb.ctl->par[level & 1].hq_cnt, make_team(blockIdx.x, gridDim.x),
                               bu_filter_level(p.bu_filter, gb.ctl->par[(level - 1) & 1].changed,
-                                              p.V));
+                                              p.V),
+                              gb.ctl->ls.smask);
+}
+
+// Sparse sources of a bottom-up level that follows a top-down one: count
+// every source's previous frontier, then pick the sparse ones (one thread).
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_dl_sparse_count(Params p, int g, CondH, CondH) {
+  const GroupBufs gb = dl_bufs(p, g);
+  Ctl* ctl = gb.ctl;
+  if (!ctl->ls.sparse_try) return;  // uniform
+  const int level = ctl->ls.level;
+  sparse_count_phase<WORDS>(p, gb, &ctl->par[level & 1], level, make_team(blockIdx.x, gridDim.x));
+}
+
+__global__ void k_dl_sparse_decide(Params p, int g, CondH, CondH) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Ctl* ctl = p.groups[g].ctl;
+  LoopState& ls = ctl->ls;
+  if (!ls.sparse_try) return;
+  const Par& pr = ctl->par[ls.level & 1];
+  const int nsrc = ls.nb;
+  unsigned long long tot = 0;
+  for (int i = 0; i < nsrc; i++) tot += pr.scnt[i];
+  uint32_t sm[kMaxWords];
+#pragma unroll
+  for (int k = 0; k < kMaxWords; k++) sm[k] = 0u;
+  for (int i = 0; i < nsrc; i++) {
+    const unsigned long long c = pr.scnt[i];
+    if (c > 0 && c * (unsigned long long)p.sparse_div * (unsigned long long)nsrc < tot)
+      sm[i >> 5] |= 1u << (i & 31);
+  }
+#pragma unroll
+  for (int k = 0; k < kMaxWords; k++) ls.smask[k] = sm[k];
+}
+
+__device__ __forceinline__ bool dl_sparse(const LoopState& ls, int words) {
+  bool any = false;
+  for (int k = 0; k < words; k++) any |= ls.smask[k] != 0u;
+  return any;
+}
+
+// After the bottom-up pass, its deferred hubs and their inspect work: the
+// sparse sources' bits, top-down (small pushers by warps, large ones queued
+// in chunks), then the chunks over all CTAs.
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_dl_push_queue(Params p, int g, CondH, CondH) {
+  const GroupBufs gb = dl_bufs(p, g);
+  Ctl* ctl = gb.ctl;
+  const LoopState& ls = ctl->ls;
+  if (!dl_sparse(ls, WORDS)) return;  // uniform
+  const int level = ls.level;
+  push_queue_phase<WORDS>(p, gb, &ctl->par[level & 1], dl_batch_size(p, ls, ls.batch), level,
+                          level <= depth_limit(p.db), ls.smask,
+                          make_team(blockIdx.x, gridDim.x));
+}
+
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_dl_push_run(Params p, int g, CondH, CondH) {
+  const GroupBufs gb = dl_bufs(p, g);
+  Ctl* ctl = gb.ctl;
+  const LoopState& ls = ctl->ls;
+  if (!dl_sparse(ls, WORDS)) return;  // uniform
+  const int level = ls.level;
+  if (ctl->par[level & 1].pq_cnt == 0) return;  // uniform
+  push_run_phase<WORDS>(p, gb, &ctl->par[level & 1], dl_batch_size(p, ls, ls.batch), level,
+                        level <= depth_limit(p.db), ls.smask, make_team(blockIdx.x, gridDim.x));
+}
+
+// After the push: clear the level+1 bitmap that the hub epilogue left
+// (it was the push's frontier); the next bottom-up pass ORs into it.
+template <int WORDS>
+__global__ void __launch_bounds__(512) k_dl_clear_next(Params p, int g, CondH, CondH) {
+  const GroupBufs gb = dl_bufs(p, g);
+  const LoopState& ls = gb.ctl->ls;
+  if (!dl_sparse(ls, WORDS)) return;  // uniform: the hub epilogue cleared it
+  zero_words(chg_at(gb, p, ls.level + 1), p.chg_stride, make_team(blockIdx.x, gridDim.x));
 }
 
 // threads per CTA and CTAs per SM of the output pass (R-MAT scale 24, one
@@ -466,6 +560,9 @@ static cudaError_t build_device_loop(const Params& p, int G, int sms, int thread
   const int gu = occ_grid((const void*)k_dl_bu<WORDS>, IBFS_DL_BU_THREADS, sms);
   const int gd = occ_grid((const void*)k_dl_bu_defer<WORDS>, threads, sms);
   const int go = occ_grid((const void*)k_dl_output<WORDS>, IBFS_DL_OUT_THREADS, sms);
+  const int gpq = occ_grid((const void*)k_dl_push_queue<WORDS>, threads, sms);
+  const int gpr = occ_grid((const void*)k_dl_push_run<WORDS>, threads, sms);
+  const int gsc = occ_grid((const void*)k_dl_sparse_count<WORDS>, threads, sms);
 #define DL_TRY(call)                   \
   do {                                 \
     e = (call);                        \
@@ -495,16 +592,30 @@ static cudaError_t build_device_loop(const Params& p, int G, int sms, int thread
     DL_TRY(dl_kernel(L, &l0, nullptr, k_dl_decide, 1, 32, p, g, hl, hd));
     cudaGraph_t S[2] = {nullptr, nullptr};
     DL_TRY(dl_cond(L, &l1, l0, hd, cudaGraphCondTypeSwitch, 2, S));
-    cudaGraphNode_t t0, t1, t2, u0, u1, u2;
+    cudaGraphNode_t t0, t1, t2, u0, u1, u2, u3, u4;
     DL_TRY(dl_kernel(S[0], &t0, nullptr, k_dl_qbuild<WORDS>, gq, threads, p, g, 0, 0));
     DL_TRY(dl_kernel(S[0], &t1, t0, k_dl_td<WORDS>, gt, threads, p, g, 0, 0));
     DL_TRY(dl_kernel(S[0], &t2, t1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
-    DL_TRY(dl_kernel(S[1], &u0, nullptr, k_dl_bu<WORDS>, gu, IBFS_DL_BU_THREADS, p, g, 0, 0));
+    cudaGraphNode_t bu_dep = nullptr;
+    if (IBFS_DL_FUSED_BU && p.sparse_div > 0) {
+      cudaGraphNode_t s0, s1;
+      DL_TRY(dl_kernel(S[1], &s0, nullptr, k_dl_sparse_count<WORDS>, gsc, threads, p, g, 0, 0));
+      DL_TRY(dl_kernel(S[1], &s1, s0, k_dl_sparse_decide, 1, 32, p, g, 0, 0));
+      bu_dep = s1;
+    }
+    DL_TRY(dl_kernel(S[1], &u0, bu_dep, k_dl_bu<WORDS>, gu, IBFS_DL_BU_THREADS, p, g, 0, 0));
     DL_TRY(dl_kernel(S[1], &u1, u0, k_dl_bu_defer<WORDS>, gd, threads, p, g, 0, 0));
-    if (IBFS_DL_FUSED_BU)
+    if (IBFS_DL_FUSED_BU) {
       DL_TRY(dl_kernel(S[1], &u2, u1, k_dl_bu_hubs<WORDS>, gh, threads, p, g, 0, 0));
-    else
+      if (p.sparse_div > 0) {
+        cudaGraphNode_t u5;
+        DL_TRY(dl_kernel(S[1], &u3, u2, k_dl_push_queue<WORDS>, gpq, threads, p, g, 0, 0));
+        DL_TRY(dl_kernel(S[1], &u4, u3, k_dl_push_run<WORDS>, gpr, threads, p, g, 0, 0));
+        DL_TRY(dl_kernel(S[1], &u5, u4, k_dl_clear_next<WORDS>, gz, threads, p, g, 0, 0));
+      }
+    } else {
       DL_TRY(dl_kernel(S[1], &u2, u1, k_dl_inspect<WORDS>, gi, threads, p, g, 0, 0));
+    }
   }
 #undef DL_TRY
   *out = top;

@@ -372,6 +372,9 @@ void fill_graph_params(const ibfs_graph* g, const ibfs_opts& o, int words, int t
   p.hub_t = kHubScan;
   p.bu_filter = o.bu_filter > 0 ? 1 : o.bu_filter == 0 ? 0 : -1;
   p.td_stage = o.td_stage > 0 ? 1 : 0;
+  // sparse-source pushes on bottom-up levels: device loop only (the caller
+  // clears it for the other schedules)
+  p.sparse_div = o.sparse_push > 0 ? o.sparse_push : 0;
   p.col_vec = 1;
   p.vmap = g->vmap.as<int32_t>();
   // Degrees are non-increasing in the internal order: the vertices above the
@@ -1010,6 +1013,7 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
   }
   Params p;
   fill_graph_params(g, o, rp.words, rp.threads, &p);
+  if (!devloop) p.sparse_div = 0;
   p.src = g->d_src.as<int32_t>();
   p.out_row = g->d_outrow.as<int32_t>();
   p.n_total = n;
@@ -1358,9 +1362,13 @@ static ibfs_status run_once(ibfs_graph* g, const int32_t* src, int64_t n, const 
     if (devloop) {
       // kernel nodes that ran: start per group; per batch init, seed,
       // inspect(0), output, end and one decide for the final level; per
-      // expanded level decide + two expand kernels + inspect
+      // expanded level decide + two expand kernels + inspect, and on
+      // bottom-up levels the sparse-source count, decision, push queue,
+      // push chunks and bitmap clear
       launches = rp.G;
-      for (int b = 0; b < rp.nbatches; b++) launches += 6 + 4LL * (br[b].td + br[b].bu);
+      const long long per_bu = p.sparse_div > 0 ? 9 : 4;
+      for (int b = 0; b < rp.nbatches; b++)
+        launches += 6 + 4LL * br[b].td + per_bu * br[b].bu;
     }
     st->gpu_launches = launches + gb_launches;
     st->device_ms = ms;

@@ -119,7 +119,14 @@ typedef struct ibfs_opts {
                               chunk in shared memory by double-buffered bulk
                               (TMA) copies (plain and device-loop schedules);
                               0 (default): reads the chunk directly              */
-    int32_t reserved[3];
+    int32_t sparse_push;   /* device loop: d > 0 makes a bottom-up level that
+                              follows a top-down one push, top-down, the sources
+                              whose previous frontier is below 1/d of the
+                              batch's average, instead of letting them hold up
+                              every vertex's early exit (exact either way).
+                              0 (default) or < 0: off.  On R-MAT scale 24 with
+                              d = 256 it measured 35.0 vs 31.1 ms per run      */
+    int32_t reserved[2];
 } ibfs_opts;
 
 typedef struct ibfs_level_rec {

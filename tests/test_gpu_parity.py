@@ -315,3 +315,26 @@ def test_top_down_staged_chunks(kind, mode, thresholds):
     src = ib.sample_sources(beg, col, 128, seed=9)
     run_and_check(beg, col, g, src, width=128, mode=mode, switch_level=2, td_stage=1,
                   sml_shed=thresholds[0], lrg_shed=thresholds[1])
+
+
+@pytest.mark.parametrize("sparse_push", [0, 256, 4, 1])
+@pytest.mark.parametrize("width", WIDTHS)
+@pytest.mark.parametrize("kind", ["rmat13", "rmat15", "grid", "chunglu"])
+def test_sparse_source_push(kind, width, sparse_push):
+    """Bottom-up levels of the device loop may hand sources with small
+    frontiers to a top-down push (exit masks without their bits): depths
+    and edge counts match the oracle whether the rule is off (0), selective
+    (256), or pushes many sources (4, and 1: every source below the average
+    frontier)."""
+    beg, col, g = graph(kind)
+    src = ib.sample_sources(beg, col, 2 * width + 5, seed=13)
+    run_and_check(beg, col, g, src, width=width, mode=ib.MODE_DEVICE_LOOP, switch_level=1,
+                  sparse_push=sparse_push)
+    res = run_and_check(beg, col, g, src, width=width, mode=ib.MODE_DEVICE_LOOP, groups=2,
+                        sparse_push=sparse_push)
+    # with the rule on, every bottom-up level also runs the count, decision,
+    # push-queue, push-chunk and bitmap-clear nodes
+    st = res.stats
+    per_bu = 9 if sparse_push > 0 else 4
+    assert st["gpu_launches"] == (st["groups"] + 6 * st["n_batches"] + 4 * st["td_levels"]
+                                  + per_bu * st["bu_levels"])
