@@ -28,6 +28,11 @@
 //   --device-loop      kernel per phase, level loop on the device (CUDA graph
 //                      conditional nodes)
 //   --batched          all batches in one launch (CUDA graph), one report
+//   --bu-filter M      bottom-up frontier filter: 1 every level, 0 off,
+//                      -1 per level (default)
+//   --td-stage         stage large vertices' chunks in shared memory (TMA)
+//   --sparse-push D    push sources below 1/D of the average frontier
+//                      top-down on a bottom-up level (default off)
 //   --repeat K         run the whole set K times (timing)
 //   --device D, --seed S, --depth-bytes 1|2, --vertex-major
 #include <chrono>
@@ -42,7 +47,8 @@
 static void usage() {
   std::printf("Input: /path/to/exe /path/to/beg /path/to/csr concurrent-count switch-level "
               "bfs_count [--sources F] [--depth-out F] [--width W] [--alpha A] [--beta B] "
-              "[--thresholds S,L] [--groupby] [--groupby-device] [--plain] [--device-loop] [--batched] [--repeat K] [--device D] "
+              "[--thresholds S,L] [--groupby] [--groupby-device] [--plain] [--device-loop] [--batched] "
+              "[--bu-filter M] [--td-stage] [--sparse-push D] [--repeat K] [--device D] "
               "[--seed S] [--depth-bytes 1|2] [--vertex-major]\n");
 }
 
@@ -94,6 +100,9 @@ int main(int argc, char** argv) {
     else if (a == "--plain") o.mode = IBFS_MODE_PLAIN;
     else if (a == "--device-loop") o.mode = IBFS_MODE_DEVICE_LOOP;
     else if (a == "--batched") batched = true;
+    else if (a == "--bu-filter") o.bu_filter = std::atoi(next("--bu-filter"));
+    else if (a == "--td-stage") o.td_stage = 1;
+    else if (a == "--sparse-push") o.sparse_push = std::atoi(next("--sparse-push"));
     else if (a == "--repeat") repeat = std::atoi(next("--repeat"));
     else if (a == "--device") device = std::atoi(next("--device"));
     else if (a == "--seed") seed = std::strtoull(next("--seed"), nullptr, 10);

@@ -31,7 +31,9 @@ def test_wrong_input_exits_like_reference():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("extra", [[], ["--groupby", "--batched"], ["--plain"],
-                                   ["--width", "64", "--alpha", "4"]])
+                                   ["--width", "64", "--alpha", "4"],
+                                   ["--device-loop", "--td-stage", "--bu-filter", "1"],
+                                   ["--device-loop", "--sparse-push", "4"]])
 def test_cli_depths_match_golden(tmp_path, extra):
     f = dict(np.load(os.path.join(HERE, "golden", "rmat_s10.npz")))
     bp, cp = str(tmp_path / "g_beg_pos.bin"), str(tmp_path / "g_csr.bin")
