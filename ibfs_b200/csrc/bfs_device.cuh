@@ -190,6 +190,7 @@ constexpr int kBuStep = IBFS_BU_STEP;
 #define IBFS_BU_PEEK 2
 #endif
 constexpr int kBuPeek = IBFS_BU_PEEK;
+
 // Bottom-up frontier filter.  A neighbour u that did not change at level L-1
 // cannot give v a bit it lacks at level L: every bit u held before L-1
 // reached v by L-1 already (BFS distances of adjacent vertices differ by at
@@ -1234,7 +1235,8 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
     }
   }
   const long long start = p.big_prefix;  // a multiple of 32
-  for (long long base = start + t.warp * 32; base < p.V; base += t.nwarps * 32) {
+  const long long rstep = t.nwarps * 32;
+  for (long long base = start + t.warp * 32; base < p.V; base += rstep) {
     const long long v = base + lane;
     const bool valid = v < p.V;
     uint32_t l[WORDS], acc[WORDS];
