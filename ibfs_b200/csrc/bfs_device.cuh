@@ -152,6 +152,10 @@ struct Params {
                     // a hub still missing bits defers the rest in chunks
   const int32_t* vmap;  // caller id -> internal id of the resident graph (null:
                         // identical); the output pass reads statuses through it
+  long long v_nz;       // bottom-up sweeps [0, v_nz): in the degree order the
+                        // vertices from v_nz on have no edges (v_nz a multiple
+                        // of 32, or V), so their statuses never change after
+                        // seeding and both status buffers agree on them
   long long big_prefix; // bottom-up: vertices [0, big_prefix) take one warp each
                         // (degree-ordered graphs: the vertices above the
                         // thread-path limit; a multiple of 32; 0 otherwise)
@@ -1236,7 +1240,16 @@ __device__ void bu_phase(const Params& p, const GroupBufs& gb, int level,
   }
   const long long start = p.big_prefix;  // a multiple of 32
   const long long rstep = t.nwarps * 32;
-  for (long long base = start + t.warp * 32; base < p.V; base += rstep) {
+  if (FUSED && first_plane) {
+    // the pass writes its first-used plane whole; the edgeless tail it does
+    // not sweep gets zeros (an edgeless source keeps depth 0)
+    const long long n4 = (p.V - p.v_nz) * WORDS / 4;
+    uint4* q = reinterpret_cast<uint4*>(gb.planes + (size_t)pb * p.plane_stride +
+                                        (size_t)p.v_nz * WORDS);
+    for (long long i = t.tid; i < n4 + ((p.V - p.v_nz) * WORDS % 4 ? 1 : 0); i += t.nthreads)
+      __stcg(q + i, make_uint4(0, 0, 0, 0));
+  }
+  for (long long base = start + t.warp * 32; base < p.v_nz; base += rstep) {
     const long long v = base + lane;
     const bool valid = v < p.V;
     uint32_t l[WORDS], acc[WORDS];

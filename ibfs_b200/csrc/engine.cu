@@ -344,6 +344,9 @@ static ibfs_status ensure_workspace(ibfs_graph* g, const RunPlan& rp, const ibfs
 
 }  // namespace ibfs
 
+#ifndef IBFS_BU_SKIP_EDGELESS
+#define IBFS_BU_SKIP_EDGELESS 1
+#endif
 namespace ibfs {
 // The launch parameters that depend only on the resident graph and the
 // options (the run's sources, rows, output, groups and records are left
@@ -385,6 +388,18 @@ void fill_graph_params(const ibfs_graph* g, const ibfs_opts& o, int words, int t
   // average out and the per-lane sweep is faster (R-MAT scale 16: 1.26 ->
   // 0.45 ms per run with the prefix pass; scale 24: 34.8 vs 40.7 ms without
   // and with it).
+  // Degrees are non-increasing in the internal order, so the edgeless
+  // vertices form a suffix: the bottom-up sweeps stop before it (rounded up
+  // to whole 32-vertex ranges).
+  {
+    int64_t lo = 0, hi = g->V;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) / 2;
+      if (g->dbeg_host[(size_t)mid + 1] - g->dbeg_host[(size_t)mid] > 0) lo = mid + 1;
+      else hi = mid;
+    }
+    p.v_nz = IBFS_BU_SKIP_EDGELESS ? std::min<int64_t>((lo + 31) & ~31LL, g->V) : g->V;
+  }
   const int64_t ranges_per_warp = ((g->V + 31) / 32) / std::max<int64_t>(1, (int64_t)g->sms * 64);
   if (ranges_per_warp < 8) {
     int64_t lo = 0, hi = g->V;
