@@ -69,6 +69,8 @@ struct LoopState {
   int32_t sync;       // the next top-down level first copies new statuses over old ones
   int32_t nb;         // sources of `batch`
   uint32_t smask[kMaxWords];  // bottom-up level: sources pushed top-down instead
+  int32_t tail_clean;         // both status buffers are zero from v_reach on
+                              // (batch_end clears its unreachable sources' words)
   int32_t sparse_try;         // this bottom-up level follows a top-down one: count
                               // the sources' frontiers and pick the sparse ones
   unsigned long long m_u, teps, prev_changed;
@@ -154,8 +156,12 @@ struct Params {
                         // identical); the output pass reads statuses through it
   long long v_nz;       // bottom-up sweeps [0, v_nz): in the degree order the
                         // vertices from v_nz on have no edges (v_nz a multiple
-                        // of 32, or V), so their statuses never change after
-                        // seeding and both status buffers agree on them
+                        // of 32, or V); a bottom-up pass cannot change them and
+                        // a top-down level (a directed graph's sinks) writes
+                        // both status buffers through inspect, so they agree
+  long long v_reach;    // v_nz when no edge points into [v_nz, V) (symmetric
+                        // graphs), else V: vertices from v_reach on are reached
+                        // only as sources, at depth 0
   long long big_prefix; // bottom-up: vertices [0, big_prefix) take one warp each
                         // (degree-ordered graphs: the vertices above the
                         // thread-path limit; a multiple of 32; 0 otherwise)
@@ -1828,20 +1834,25 @@ __device__ void output_sm_u8(const Params& p, const GroupBufs& gb, const int32_t
       for (int i = 0; i < 4; i++) {
         const bool in = v0 + i < p.V;
         const size_t vi = vis[i];
+        // a vertex from v_reach on is reached only as a source, at depth 0:
+        // its plane words are zeros (every plane was first written whole
+        // during the batch), so they are not gathered
+        const bool edged = in && (long long)vi < p.v_reach;
         const uint32_t nst = in ? ~gb.last[vi * WORDS + k] : 0xFFFFFFFFu;
         if constexpr (NP <= 7) {
           // planes in rows 0..NP-1, zero rows up to 6 (folded away by the
           // compiler), the unreached flag in row 7
 #pragma unroll
           for (int b = 0; b < 7; b++)
-            A[8 * i + b] = (b < NP && in) ? gb.planes[(size_t)b * p.plane_stride + vi * WORDS + k]
-                                          : 0u;
+            A[8 * i + b] = (b < NP && edged)
+                               ? gb.planes[(size_t)b * p.plane_stride + vi * WORDS + k]
+                               : 0u;
           A[8 * i + 7] = nst;
         } else {
 #pragma unroll
           for (int b = 0; b < 8; b++) {
             uint32_t x = 0u;
-            if (in) x = gb.planes[(size_t)b * p.plane_stride + vi * WORDS + k];
+            if (edged) x = gb.planes[(size_t)b * p.plane_stride + vi * WORDS + k];
             A[8 * i + b] = x | nst;
           }
         }

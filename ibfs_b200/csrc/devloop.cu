@@ -175,7 +175,10 @@ constexpr int kDlLoopThreads = 128;
 __global__ void k_dl_start(Params p, int g, CondH h_batch, CondH) {
   if (blockIdx.x != 0) return;
   Ctl* ctl = p.groups[g].ctl;
-  if (threadIdx.x == 0) ctl->ls.err = 0;
+  if (threadIdx.x == 0) {
+    ctl->ls.err = 0;
+    ctl->ls.tail_clean = 0;  // the first batch of the launch zeroes everything
+  }
   const bool go = dl_next_batch(p, ctl, g, -1);
   if (threadIdx.x == 0) cudaGraphSetConditional(h_batch, go ? 1u : 0u);
 }
@@ -187,8 +190,11 @@ __global__ void __launch_bounds__(512) k_dl_batch_init(Params p, int g, CondH h_
   const GroupBufs gb = p.groups[g];
   const Team t = make_team(blockIdx.x, gridDim.x);
   const long long vpad = (p.V + 31) & ~31LL;
-  zero_words(gb.last, vpad * WORDS, t);
-  zero_words(gb.curr, vpad * WORDS, t);
+  // after the group's first batch of a launch the statuses from v_reach on
+  // are already zero (the previous batch cleared its sources' words there)
+  const long long zv = (gb.ctl->ls.tail_clean && p.v_reach < p.V) ? p.v_reach : vpad;
+  zero_words(gb.last, zv * WORDS, t);
+  zero_words(gb.curr, zv * WORDS, t);
   zero_words(gb.chg, 2 * p.chg_stride, t);
   if (t.tid == 0) {
     Ctl* ctl = gb.ctl;
@@ -479,8 +485,24 @@ __global__ void k_dl_batch_end(Params p, int g, CondH h_batch, CondH) {
   Ctl* ctl = p.groups[g].ctl;
   LoopState& ls = ctl->ls;
   const int b = ls.batch;
+  // the batch's sources from v_reach on were the only nonzero status words
+  // there: clear them for the group's next batch
+  if (p.v_reach < p.V) {
+    const GroupBufs& gb = p.groups[g];
+    const long long words = p.plane_stride / ((p.V + 31) & ~31LL);  // status words per vertex
+    for (int j = threadIdx.x; j < ls.nb; j += blockDim.x) {
+      const int32_t v = p.src[(size_t)b * p.C + j];
+      if (v < p.v_reach) continue;
+      for (long long k = 0; k < words; k++) {
+        gb.last[(size_t)v * words + k] = 0u;
+        gb.curr[(size_t)v * words + k] = 0u;
+      }
+    }
+  }
   __shared__ int s_stop;
+  __syncthreads();
   if (threadIdx.x == 0) {
+    ls.tail_clean = 1;
     s_stop = 0;
     if (ls.err && p.q_slots > 0) {
       // serving: the error belongs to this batch's queries alone; report it

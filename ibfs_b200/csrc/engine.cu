@@ -198,6 +198,7 @@ struct ibfs_graph {
   DevBuf vmap;          // caller id -> internal id (device)
   std::vector<int32_t> new_of_old;  // the same on the host
   std::vector<int64_t> dbeg_host;   // offsets of the internal (degree-ordered) CSR
+  int64_t col_max = -1;             // largest neighbour id of the internal CSR
   DevBuf gbin, gbkeys;  // device GroupBy: caller-order sources, sort keys
   int64_t defer_cap = 16;  // bound on deferred bottom-up hub chunks per level
   cudaStream_t own_stream = nullptr;
@@ -399,6 +400,9 @@ void fill_graph_params(const ibfs_graph* g, const ibfs_opts& o, int words, int t
       else hi = mid;
     }
     p.v_nz = IBFS_BU_SKIP_EDGELESS ? std::min<int64_t>((lo + 31) & ~31LL, g->V) : g->V;
+    // no edge points into the edgeless suffix (symmetric graphs): only a
+    // source reaches a vertex there (a directed graph's sinks can be reached)
+    p.v_reach = g->col_max < p.v_nz ? p.v_nz : g->V;
   }
   const int64_t ranges_per_warp = ((g->V + 31) / 32) / std::max<int64_t>(1, (int64_t)g->sms * 64);
   if (ranges_per_warp < 8) {
@@ -555,14 +559,17 @@ static ibfs_status upload_graph(ibfs_graph* g) {
       nbeg[(size_t)i + 1] = nbeg[(size_t)i] + (bg[o + 1] - bg[o]);
     }
     const int32_t* nmap = g->new_of_old.data();
-#pragma omp parallel for schedule(dynamic, 4096)
+    int64_t col_max = -1;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(max : col_max)
     for (int64_t i = 0; i < g->V; i++) {
       const int32_t o = order[(size_t)i];
       int32_t* out = dcol.data() + nbeg[(size_t)i];
       const int64_t d = bg[o + 1] - bg[o];
       for (int64_t e = 0; e < d; e++) out[e] = nmap[cl[bg[o] + e]];
       std::sort(out, out + d);
+      if (d > 0) col_max = std::max<int64_t>(col_max, out[d - 1]);
     }
+    g->col_max = col_max;
     CU(cudaMemcpyAsync(g->beg.p, nbeg.data(), sizeof(int64_t) * (size_t)(g->V + 1),
                        cudaMemcpyHostToDevice, g->stream));
     g->dbeg_host = nbeg;  // (the copy is synchronised below)

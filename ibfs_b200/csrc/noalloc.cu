@@ -138,6 +138,7 @@ extern "C" ibfs_status ibfs_run_static_scratch(const int64_t* beg_dev, const int
   p.col = col_dev;
   p.V = V;
   p.v_nz = V;  // the caller's CSR is not degree-ordered: sweep every vertex
+  p.v_reach = V;
   p.E = E;
   p.nchg = (V + 31) / 32;
   p.chg_stride = (long long)nchg;

@@ -338,3 +338,62 @@ def test_sparse_source_push(kind, width, sparse_push):
     per_bu = 9 if sparse_push > 0 else 4
     assert st["gpu_launches"] == (st["groups"] + 6 * st["n_batches"] + 4 * st["td_levels"]
                                   + per_bu * st["bu_levels"])
+
+
+@pytest.mark.parametrize("groups", [1, 2])
+def test_edgeless_sources_across_batches(groups):
+    """Edgeless vertices sit at the end of the internal degree order and are
+    skipped by the bottom-up sweeps; the device loop then zeroes only the
+    rest of the status buffers per batch and clears each batch's edgeless
+    sources itself.  Many batches in one group, most sources edgeless, two
+    runs in a row: every depth must still be exact."""
+    beg0, col0 = ib.gen_rmat(12, 8, seed=21)
+    deg = np.diff(beg0)
+    iso = np.nonzero(deg == 0)[0].astype(np.int32)
+    assert len(iso) > 200
+    g = ib.Graph.from_csr(beg0, col0)
+    try:
+        nz = ib.sample_sources(beg0, col0, 60, seed=22)
+        rng = np.random.default_rng(23)
+        src = np.concatenate([iso[rng.integers(0, len(iso), 200)], nz]).astype(np.int32)
+        rng.shuffle(src)
+        for _ in range(2):
+            run_and_check(beg0, col0, g, src, width=32, mode=ib.MODE_DEVICE_LOOP, groups=groups,
+                          switch_level=1)
+            run_and_check(beg0, col0, g, src[:37], width=32, mode=ib.MODE_DEVICE_LOOP,
+                          groups=groups, switch_level=1)
+    finally:
+        g.close()
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_directed_sinks_reached(mode):
+    """A directed CSR whose second half has no out-edges but is pointed to:
+    those sinks sit in the edgeless suffix of the degree order yet are
+    reached at depths above 0, so neither the output pass nor the per-batch
+    zeroing may treat that suffix as source-only.  Top-down only (a directed
+    BFS; the bottom-up step reads the same lists as in-edges, which holds for
+    symmetric graphs alone)."""
+    rng = np.random.default_rng(31)
+    V, H = 3000, 1500
+    lists = []
+    for v in range(V):
+        if v >= H:
+            lists.append(np.zeros(0, np.int32))
+            continue
+        nb = np.unique(rng.integers(0, V, 6 + (v % 11)).astype(np.int32))
+        lists.append(nb[nb != v])
+    beg = np.zeros(V + 1, np.int64)
+    beg[1:] = np.cumsum([len(x) for x in lists])
+    col = np.concatenate(lists).astype(np.int32)
+    g = ib.Graph.from_csr(beg, col)
+    try:
+        src = np.concatenate([rng.integers(0, H, 70), rng.integers(H, V, 10)]).astype(np.int32)
+        for groups in (1, 2):
+            for _ in range(2):
+                res = run_and_check(beg, col, g, src, width=32, mode=mode, groups=groups,
+                                    switch_level=250)
+                assert res.stats["bu_levels"] == 0
+                assert int((res.depth[:, H:] != 0xFF).sum()) > 1000
+    finally:
+        g.close()
