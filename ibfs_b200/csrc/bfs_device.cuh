@@ -1804,6 +1804,56 @@ __device__ __forceinline__ void transpose32(uint32_t (&A)[32]) {
   }
 }
 
+#ifndef IBFS_OUT_PRMT
+#define IBFS_OUT_PRMT 1
+#endif
+
+// The same transpose with its first two rounds (whole 16- and 8-bit blocks)
+// as byte permutes, two per row pair instead of a five-instruction masked
+// delta swap.  Z: bit r set = row r is zero on entry (a compile-time
+// constant), so that pairs of zero rows are skipped; the rounds commute, so
+// the order of the five does not matter.
+template <uint32_t Z>
+__device__ __forceinline__ void transpose32_z(uint32_t (&A)[32]) {
+#pragma unroll
+  for (int r = 0; r < 16; r++) {
+    if (((Z >> r) & 1u) && ((Z >> (r + 16)) & 1u)) continue;
+    const uint32_t a = A[r], b = A[r + 16];
+    A[r] = __byte_perm(a, b, 0x5410);       // low halves
+    A[r + 16] = __byte_perm(a, b, 0x7632);  // high halves
+  }
+  constexpr uint32_t Z1 = (Z & (Z >> 16) & 0xFFFFu) * 0x10001u;
+#pragma unroll
+  for (int r = 0; r < 32; r++) {
+    if (r & 8) continue;
+    if (((Z1 >> r) & 1u) && ((Z1 >> (r + 8)) & 1u)) continue;
+    const uint32_t a = A[r], b = A[r + 8];
+    A[r] = __byte_perm(a, b, 0x6240);      // bytes 0 and 2 of both
+    A[r + 8] = __byte_perm(a, b, 0x7351);  // bytes 1 and 3 of both
+  }
+#pragma unroll
+  for (int lv = 2; lv < 5; lv++) {
+    const int j = 16 >> lv;
+    const uint32_t m = lv == 2 ? 0x0F0F0F0Fu : lv == 3 ? 0x33333333u : 0x55555555u;
+#pragma unroll
+    for (int r = 0; r < 32; r++) {
+      if (r & j) continue;
+      const uint32_t t = ((A[r] >> j) ^ A[r + j]) & m;
+      A[r + j] ^= t;
+      A[r] ^= t << j;
+    }
+  }
+}
+
+// Rows known zero in output_sm_u8's matrix: 8i + b for NP <= b <= 6.
+template <int NP>
+__host__ __device__ constexpr uint32_t out_zero_rows() {
+  uint32_t z = 0u;
+  for (int i = 0; i < 4; i++)
+    for (int b = NP; b < 7; b++) z |= 1u << (8 * i + b);
+  return z;
+}
+
 // Source-major, one-byte depths, NP (<= 8) planes known at compile time:
 // lane = 4 consecutive vertices, one 4-byte store per source row.  The
 // depth byte of (vertex i, source s) has bit b = bit s of plane b of vertex
@@ -1857,7 +1907,11 @@ __device__ void output_sm_u8(const Params& p, const GroupBufs& gb, const int32_t
           }
         }
       }
+#if IBFS_OUT_PRMT
+      transpose32_z<out_zero_rows<NP>()>(A);
+#else
       transpose32(A);
+#endif
       if constexpr (NP <= 7) {
         // byte i = depth (< 128) with bit 7 = unreached: widen bit 7 to the
         // whole byte (prmt in sign-replicating mode), 0xFF = INFTY
