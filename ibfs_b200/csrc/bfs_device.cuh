@@ -1807,6 +1807,24 @@ __device__ __forceinline__ void transpose32(uint32_t (&A)[32]) {
 #ifndef IBFS_OUT_PRMT
 #define IBFS_OUT_PRMT 1
 #endif
+#ifndef IBFS_OUT_FASTST
+#define IBFS_OUT_FASTST 1
+#endif
+#ifndef IBFS_OUT_STCS
+#define IBFS_OUT_STCS 1
+#endif
+
+// A 4-byte piece of a depth row.  The rows are written once and not read
+// again on the device: with IBFS_OUT_STCS they are streaming stores (evict
+// first), so that they do not push the gathered statuses and planes out of
+// L2.
+__device__ __forceinline__ void st_row4(uint8_t* a, uint32_t x) {
+#if IBFS_OUT_STCS
+  __stcs(reinterpret_cast<unsigned int*>(a), x);
+#else
+  *reinterpret_cast<uint32_t*>(a) = x;
+#endif
+}
 
 // The same transpose with its first two rounds (whole 16- and 8-bit blocks)
 // as byte permutes, two per row pair instead of a five-instruction masked
@@ -1838,9 +1856,11 @@ __device__ __forceinline__ void transpose32_z(uint32_t (&A)[32]) {
 #pragma unroll
     for (int r = 0; r < 32; r++) {
       if (r & j) continue;
-      const uint32_t t = ((A[r] >> j) ^ A[r + j]) & m;
-      A[r + j] ^= t;
-      A[r] ^= t << j;
+      // m << j == ~m: each row keeps its own half and takes the partner's
+      // other half, a shift and a three-input select each
+      const uint32_t a = A[r], b = A[r + j];
+      A[r] = (a & m) | ((b << j) & ~m);
+      A[r + j] = ((a >> j) & m) | (b & ~m);
     }
   }
 }
@@ -1923,12 +1943,21 @@ __device__ void output_sm_u8(const Params& p, const GroupBufs& gb, const int32_t
         }
       }
       const int js = min(32, n_b - k * 32);
+#if IBFS_OUT_FASTST
+      if (full4 && js == 32) {
+        // the common case: 32 whole rows, 4 in-range vertices per lane
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+          st_row4(p.out + (size_t)rows[k * 32 + j] * (size_t)p.V + v0, A[j]);
+        continue;
+      }
+#endif
 #pragma unroll
       for (int j = 0; j < 32; j++) {
         if (j < js) {
           uint8_t* row = p.out + (size_t)rows[k * 32 + j] * (size_t)p.V;
           if (full4) {
-            *reinterpret_cast<uint32_t*>(row + v0) = A[j];
+            st_row4(row + v0, A[j]);
           } else {
             for (int i = 0; i < 4; i++)
               if (v0 + i < p.V) row[v0 + i] = (uint8_t)(A[j] >> (8 * i));
